@@ -1,0 +1,188 @@
+/* vfray_b200: the VF-Ray render path on B200 (sm_100a), behind a C ABI.
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status
+ * (VFR_OK = 0, negative on error) and never aborts; vfr_last_error() gives the
+ * message of the last failure on a context.  A context is used by one host
+ * thread at a time; all GPU work of a context is ordered on its stream.
+ *
+ * The array layouts at this boundary are the reference's own
+ * (vfRayKernelCPU.h:61-80, vfRayPreComp.h:83-94): vertices are float4
+ * (x, y, z, s), tets are uint4 vertex ids, the adjacency `conTet` is uint4
+ * neighbour ids with the tet's own id marking a boundary face, external faces
+ * are uint2 (tet, face), where face f of a tet is its vertices
+ * (f, f+1, f+2) mod 4.  The transfer function is 256 x RGBA float and the
+ * partial pre-integration table is 512 x 512 float indexed [front][back]
+ * (psiGammaTable512.h:10-20).  Images are row-major with row = pixel y,
+ * RGB8 as the reference writes them (vfRayKernelCPU.cc:550-552).
+ */
+#ifndef VFRAY_H
+#define VFRAY_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define VFR_API __attribute__((visibility("default")))
+#else
+#define VFR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VFR_OK 0
+#define VFR_ERR_INVALID (-1)  /* bad argument or size */
+#define VFR_ERR_CUDA (-2)     /* CUDA runtime error */
+#define VFR_ERR_MESH (-3)     /* mesh failed validation */
+#define VFR_ERR_NOMEM (-4)    /* device or host allocation failed */
+#define VFR_ERR_DEVICE (-5)   /* a kernel reported an error in the status word */
+#define VFR_ERR_STATE (-6)    /* call out of order / unknown handle */
+#define VFR_ERR_IO (-7)       /* file could not be read or written */
+#define VFR_ERR_BUDGET (-8)   /* request exceeds the memory budget */
+#define VFR_ERR_TIMEOUT (-9)  /* a bounded device wait gave up */
+
+/* Device status word bits (vfr_render_stats.device_status). */
+#define VFR_DEV_ABANDON 1u    /* adjacency did not point back (reference :365 return) */
+#define VFR_DEV_STEP_CAP 2u   /* a ray hit the per-ray step cap */
+#define VFR_DEV_RANGE 4u      /* an id read on the device was out of range */
+#define VFR_DEV_QUEUE 8u      /* a bounded work-queue wait gave up */
+#define VFR_DEV_OVERFLOW 16u  /* an entry list exceeded its capacity */
+
+/* Render modes. */
+#define VFR_MODE_REF 0        /* reference semantics: last visible face wins each pixel */
+#define VFR_MODE_COMPOSITED 1 /* depth-ordered entry lists; segments composited */
+
+typedef struct vfr_ctx vfr_ctx;
+
+typedef struct {
+  uint32_t num_ext;        /* external faces */
+  uint32_t num_vis;        /* visible faces (without the reference's padding duplicate) */
+  uint32_t num_rays;       /* pixels with an entry face */
+  uint32_t num_entries;    /* entry-list entries (composited mode) */
+  uint64_t num_steps;      /* tet-walk iterations over all rays */
+  uint32_t device_status;  /* VFR_DEV_* bits */
+  float ms_visible;        /* stage (a) device time */
+  float ms_project;        /* stage (b) device time */
+  float ms_traverse;       /* stage (c) device time */
+  float ms_total;          /* all three, device time */
+} vfr_render_stats;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Replaces the reference's initCUDA (vfRay.cu:256-288) and its globals
+ * (vfRay.cu:110-151): one context per device. */
+VFR_API int vfr_create(vfr_ctx** ctx, int device);
+VFR_API void vfr_destroy(vfr_ctx* ctx);
+VFR_API const char* vfr_last_error(const vfr_ctx* ctx);
+VFR_API const char* vfr_status_string(int status);
+/* Use a caller-owned cudaStream_t (NULL: the context's own stream). */
+VFR_API int vfr_set_stream(vfr_ctx* ctx, void* stream);
+VFR_API int vfr_synchronize(vfr_ctx* ctx);
+
+/* ---- tables (vfRay.cu:266-285 uploads the TF and the psi cudaArray) ---- */
+
+/* tf256x4: 256 RGBA entries (vfRayPreComp.cc:551-579 reads them).
+ * psi512x512: the psi(gamma) table, [front][back]; NULL selects the table
+ * this library generates (see vfr_psi_table). */
+VFR_API int vfr_tables_upload(vfr_ctx* ctx, const float* tf256x4, const float* psi512x512);
+
+/* ---- meshes ------------------------------------------------------------ */
+
+/* Replaces prepareDevice1 + the initCUDA uploads (vfRay.cu:256-307).  The
+ * arrays are copied; the mesh stays resident until released.  Validates ids,
+ * adjacency symmetry and the external-face list (VFR_ERR_MESH on failure:
+ * the reference would walk such a mesh into its :365 `return`).  maxZ/minZ
+ * are accepted for the .lmt layout; only maxEdge enters the render. */
+VFR_API int vfr_mesh_upload(vfr_ctx* ctx, const float* vert4, uint32_t nV, const uint32_t* tet4,
+                    const uint32_t* con4, uint32_t nT, const uint32_t* extf2, uint32_t nExt,
+                    float maxEdge, float maxZ, float minZ, int* mesh_id);
+VFR_API int vfr_mesh_release(vfr_ctx* ctx, int mesh_id);
+/* Device bytes the mesh holds (records, vertices, external faces). */
+VFR_API int vfr_mesh_bytes(vfr_ctx* ctx, int mesh_id, uint64_t* bytes);
+
+/* ---- the three stages, one view --------------------------------------- */
+
+/* Stage (a): findVisibleFaces + compaction (vfRayKernel.cu:70-168 and the
+ * host loop vfRay.cu:345-404; CPU twin vfRayKernelCPU.cc:51-132, main.cc:73-146).
+ * Optional host outputs: visExt (ext-face index of each visible face in
+ * order, capacity nExt), faceData (nExt x 6 floats: zParams, sParams, with
+ * sParams.x = -1 marking back faces exactly as the reference does). */
+VFR_API int vfr_find_visible(vfr_ctx* ctx, int mesh_id, uint32_t* num_vis, uint32_t* visExt,
+                     float* faceData);
+
+/* Stage (b): projectVisibleFaces + per-pixel entry faces (vfRayKernel.cu:171-228;
+ * CPU vfRayKernelCPU.cc:136-169, main.cc:164-182).  Needs stage (a) of the
+ * same mesh first.  Optional host outputs: bbox (4 per visible face:
+ * xmin, ymin, xmax, ymax) and writer (W*H ext-face index of the face whose
+ * ray the reference writes last at each pixel, -1 for none). */
+VFR_API int vfr_project(vfr_ctx* ctx, int mesh_id, uint32_t W, uint32_t H, uint32_t* bbox,
+                int32_t* writer);
+
+/* Stage (c): traversal + compositing (vfRayKernel.cu:231-852; CPU
+ * vfRayKernelCPU.cc:173-566).  Needs stage (b) first.  Optional host
+ * outputs: rgb8 (W*H*3), rgba (W*H*4 float: clamped colour, alpha = 1 - prod
+ * zeta), steps (W*H tet-walk iterations of each pixel's ray). */
+VFR_API int vfr_traverse(vfr_ctx* ctx, int mesh_id, uint8_t* rgb8, float* rgba, uint32_t* steps,
+                 vfr_render_stats* stats);
+
+/* All three stages of one view in one call, host outputs (any may be NULL).
+ * mv16: optional row-major 4x4 model-view applied as rotateVolume +
+ * normalizeVertices + buildLmt of the view on the device (vfRayPreComp.cc:84-145,
+ * 808-853, 886-906); NULL renders the mesh as uploaded with its uploaded
+ * maxEdge.  mode: VFR_MODE_REF or VFR_MODE_COMPOSITED. */
+VFR_API int vfr_render(vfr_ctx* ctx, int mesh_id, const float* mv16, uint32_t W, uint32_t H, int mode,
+               uint8_t* rgb8, float* rgba, uint32_t* steps, vfr_render_stats* stats);
+
+/* Same, but asynchronous on the context stream with device outputs (any may
+ * be NULL); stats are not filled.  Call vfr_synchronize, then
+ * vfr_device_status, before reading the outputs. */
+VFR_API int vfr_render_device(vfr_ctx* ctx, int mesh_id, const float* mv16, uint32_t W, uint32_t H,
+                      int mode, uint8_t* rgb8_dev, float* rgba_dev, uint32_t* steps_dev,
+                      int32_t* writer_dev);
+VFR_API int vfr_device_status(vfr_ctx* ctx, uint32_t* status);
+
+/* ---- host-side precomputation and files (vfRayPreComp.h:97-279) -------- */
+
+/* The psi(gamma) table this library generates: psi(tf, tb) =
+ * int_0^1 exp(-(tf*u + (tb - tf)*u^2/2)) du at gamma = i/512, tau =
+ * gamma/(1-gamma), truncated to 7 decimals like psiGammaTable512.h. */
+VFR_API int vfr_psi_table(float* out512x512);
+/* normalizeVertices (vfRayPreComp.cc:84-145), in place. */
+VFR_API int vfr_normalize(float* vert4, uint32_t nV);
+/* rotateVolume (vfRayPreComp.cc:886-906), in place; mv16 row-major. */
+VFR_API int vfr_rotate(float* vert4, uint32_t nV, const float* mv16);
+/* buildIncid + buildCon (vfRayPreComp.cc:219-501) by hashing sorted face
+ * triples: the same neighbour ids, O(nT log nT).  con4: nT*4 out. */
+VFR_API int vfr_build_con(const uint32_t* tet4, uint32_t nT, uint32_t nV, uint32_t* con4,
+                  uint32_t* num_ext, int threads);
+/* buildExtF (vfRayPreComp.cc:710-737): (tet, face) pairs, tet-then-face order. */
+VFR_API int vfr_build_extf(const uint32_t* con4, uint32_t nT, uint32_t* extf2, uint32_t cap,
+                   uint32_t* num_ext);
+/* buildLmt (vfRayPreComp.cc:808-853): out3 = maxEdgeLength, maxZ, minZ. */
+VFR_API int vfr_build_lmt(const float* vert4, uint32_t nV, const uint32_t* tet4, uint32_t nT,
+                  float* out3);
+/* buildTF (vfRayPreComp.cc:595-622): the 4-band default transfer function. */
+VFR_API int vfr_default_tf(float* tf256x4);
+
+/* Readers/writers in the reference text formats (vfRayPreComp.cc:29-880).
+ * Readers are two-step: call with NULL buffers to get the sizes. */
+VFR_API int vfr_read_off(const char* path, float* vert4, uint32_t* nV, uint32_t* tet4, uint32_t* nT);
+VFR_API int vfr_read_con(const char* path, uint32_t* con4, uint32_t* nT, uint32_t* num_ext);
+VFR_API int vfr_read_extf(const char* path, uint32_t* extf2, uint32_t* num_ext);
+VFR_API int vfr_read_lmt(const char* path, float* out3);
+VFR_API int vfr_read_tf(const char* path, float* tf256x4);
+VFR_API int vfr_write_off(const char* path, const float* vert4, uint32_t nV, const uint32_t* tet4,
+                  uint32_t nT);
+VFR_API int vfr_write_con(const char* path, const uint32_t* con4, uint32_t nT, uint32_t num_ext);
+VFR_API int vfr_write_extf(const char* path, const uint32_t* extf2, uint32_t num_ext);
+VFR_API int vfr_write_lmt(const char* path, const float* in3);
+VFR_API int vfr_write_tf(const char* path, const float* tf256x4);
+/* ppmWrite (vfRayPreComp.cc:915-934): P6, RGB8. */
+VFR_API int vfr_write_ppm(const char* path, const uint8_t* rgb8, uint32_t W, uint32_t H);
+/* Parse a psiGammaTable512.h-style C source ("float name[512][512] = {...}"). */
+VFR_API int vfr_read_psi_source(const char* path, float* out512x512);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,100 @@
+"""The CPU oracle (oracle/vfr_oracle.c) against the reference: the committed
+golden fixtures (produced by the reference's own kernels) and, where the
+reference sources are present, the reference built here."""
+import numpy as np
+import pytest
+
+from vfray_b200 import synth
+from tests.conftest import GOLDEN_CASES, has_reference_sources, load_golden
+
+needs_ref = pytest.mark.skipif(not has_reference_sources(), reason="reference sources absent")
+
+
+def oracle_mesh(Or, d, psi=None):
+    return Or.mesh(d["vert"], d["tet"], d["con"], d["extf"], d["tf"],
+                   d["psi"] if psi is None else psi, d["lmt"][0])
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_matches_golden(name, oracle_lib):
+    d = load_golden(name)
+    m = oracle_mesh(oracle_lib, d)
+    o = oracle_lib.render_ref(m, d["W"], d["H"])
+    _, vis = oracle_lib.find_visible(m)
+    assert np.array_equal(vis, d["vis"])                      # visible set, in order
+    assert np.array_equal(oracle_lib.project(m, vis, d["W"], d["H"]), d["bbox"])
+    assert np.array_equal(o["writer"], d["writer"])           # per-pixel entry face
+    assert np.array_equal(o["face_comp"], d["face_comp"])     # compositing steps per face
+    assert np.array_equal(o["rgb8"], d["rgb8"])               # image, bit for bit
+    assert np.array_equal(oracle_lib.winners(m, d["W"], d["H"]), d["writer"])
+
+
+# Pixels beyond 2/255 between the reference built with its own flags
+# (-O3 -ffast-math, g++ 13.3) and the IEEE build, as generated.  Fast-math
+# lets the compiler reassociate the edge tests and the scalar interpolation,
+# so rays flip exit faces on degenerate (axis-aligned) faces and TF lookups
+# flip across the alpha cutoff.  The IEEE build is the parity target.
+FASTMATH_BEYOND_2 = {"convex6_rot": 0, "carved10_rot": 0, "convex5_axis": 28, "single_tet": 0,
+                     "cfg0_convex24": 3}
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_fastmath_reference_deviation_is_pinned(name):
+    d = load_golden(name)
+    diff = np.abs(d["rgb8"].astype(int) - d["rgb8_fastmath"].astype(int)).max(-1)
+    assert (diff > 2).sum() == FASTMATH_BEYOND_2[name]
+
+
+def test_trace_pixels_matches_render(oracle_lib):
+    d = load_golden("carved10_rot")
+    m = oracle_mesh(oracle_lib, d)
+    o = oracle_lib.render_ref(m, d["W"], d["H"])
+    pix = np.flatnonzero(o["writer"].ravel() >= 0).astype(np.uint32)
+    t = oracle_lib.trace_pixels(m, d["W"], d["H"], pix, o["writer"].ravel()[pix], threads=2)
+    assert t["status"] == 0
+    assert np.array_equal(t["rgb8"], o["rgb8"].reshape(-1, 3)[pix])
+    assert np.array_equal(t["steps"], o["steps"].ravel()[pix])
+
+
+def test_composited_equals_single_segment_on_convex(oracle_lib):
+    """On a convex mesh every ray has one segment; the composited mode gives
+    the reference image except where the reference's column break or a
+    shared-edge tie picks another face."""
+    d = load_golden("convex6_rot")
+    m = oracle_mesh(oracle_lib, d)
+    o = oracle_lib.render_ref(m, d["W"], d["H"])
+    c = oracle_lib.render_composited(m, d["W"], d["H"], threads=2)
+    assert c["status"] >= 0 and c["nseg"].max() <= 1
+    same = (o["rgb8"] == c["rgb8"]).all(-1)
+    assert same.mean() > 0.98
+
+
+def test_composited_reenters_carved(oracle_lib):
+    d = load_golden("carved10_rot")
+    c = oracle_lib.render_composited(oracle_mesh(oracle_lib, d), d["W"], d["H"], threads=2)
+    assert c["nseg"].max() >= 2        # some rays leave and re-enter the mesh
+    assert c["status"] >= 0
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [21, 22, 23])
+def test_oracle_matches_live_reference(seed, oracle_lib):
+    import oracle
+
+    vert, tet = synth.make_mesh(9, carved=bool(seed % 2), view_seed=seed)
+    tf = synth.transfer_function(seed)
+    R = oracle.Reference("count")
+    R.set_mesh(vert, tet)
+    R.normalize()
+    R.build_con()
+    R.build_extf()
+    R.build_lmt()
+    psi = R.psi()  # the reference's own table this time
+    con, ne = R.con()
+    R.set_tf(tf)
+    r = R.render(80, 64)
+    m = oracle_lib.mesh(R.vert(), tet, con, R.extf(), tf, psi, R.lmt()[0])
+    o = oracle_lib.render_ref(m, 80, 64)
+    assert np.array_equal(o["rgb8"], r["rgb8"])
+    assert np.array_equal(o["writer"], r["writer"])
+    assert np.array_equal(o["face_comp"], r["face_exp"])

@@ -1,0 +1,143 @@
+"""ctypes binding of the vfray_b200 C ABI (include/vfray.h).
+
+The shared library is built in-tree (``make -C vfray_b200`` or
+``__graft_entry__.build()``) as vfray_b200/libvfray_b200.so.  There is no
+fallback: if the library is missing, or a call fails, this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvfray_b200.so")
+
+VFR_OK = 0
+VFR_ERR_INVALID = -1
+VFR_ERR_CUDA = -2
+VFR_ERR_MESH = -3
+VFR_ERR_NOMEM = -4
+VFR_ERR_DEVICE = -5
+VFR_ERR_STATE = -6
+VFR_ERR_IO = -7
+VFR_ERR_BUDGET = -8
+VFR_ERR_TIMEOUT = -9
+
+VFR_DEV_ABANDON = 1
+VFR_DEV_STEP_CAP = 2
+VFR_DEV_RANGE = 4
+VFR_DEV_QUEUE = 8
+VFR_DEV_OVERFLOW = 16
+
+MODE_REF = 0
+MODE_COMPOSITED = 1
+
+
+class VfrError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("num_ext", C.c_uint32), ("num_vis", C.c_uint32), ("num_rays", C.c_uint32),
+                ("num_entries", C.c_uint32), ("num_steps", C.c_uint64),
+                ("device_status", C.c_uint32), ("ms_visible", C.c_float),
+                ("ms_project", C.c_float), ("ms_traverse", C.c_float), ("ms_total", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_vp = C.c_void_p
+_u32 = C.c_uint32
+_i = C.c_int
+_f = C.c_float
+
+# name -> (restype, argtypes); mirrors include/vfray.h
+SIGNATURES = {
+    "vfr_create": (_i, [C.POINTER(_vp), _i]),
+    "vfr_destroy": (None, [_vp]),
+    "vfr_last_error": (C.c_char_p, [_vp]),
+    "vfr_status_string": (C.c_char_p, [_i]),
+    "vfr_set_stream": (_i, [_vp, _vp]),
+    "vfr_synchronize": (_i, [_vp]),
+    "vfr_tables_upload": (_i, [_vp, _vp, _vp]),
+    "vfr_mesh_upload": (_i, [_vp, _vp, _u32, _vp, _vp, _u32, _vp, _u32, _f, _f, _f,
+                             C.POINTER(_i)]),
+    "vfr_mesh_release": (_i, [_vp, _i]),
+    "vfr_mesh_bytes": (_i, [_vp, _i, C.POINTER(C.c_uint64)]),
+    "vfr_find_visible": (_i, [_vp, _i, C.POINTER(_u32), _vp, _vp]),
+    "vfr_project": (_i, [_vp, _i, _u32, _u32, _vp, _vp]),
+    "vfr_traverse": (_i, [_vp, _i, _vp, _vp, _vp, C.POINTER(RenderStats)]),
+    "vfr_render": (_i, [_vp, _i, _vp, _u32, _u32, _i, _vp, _vp, _vp, C.POINTER(RenderStats)]),
+    "vfr_render_device": (_i, [_vp, _i, _vp, _u32, _u32, _i, _vp, _vp, _vp, _vp]),
+    "vfr_device_status": (_i, [_vp, C.POINTER(_u32)]),
+    "vfr_psi_table": (_i, [_vp]),
+    "vfr_normalize": (_i, [_vp, _u32]),
+    "vfr_rotate": (_i, [_vp, _u32, _vp]),
+    "vfr_build_con": (_i, [_vp, _u32, _u32, _vp, C.POINTER(_u32), _i]),
+    "vfr_build_extf": (_i, [_vp, _u32, _vp, _u32, C.POINTER(_u32)]),
+    "vfr_build_lmt": (_i, [_vp, _u32, _vp, _u32, _vp]),
+    "vfr_default_tf": (_i, [_vp]),
+    "vfr_read_off": (_i, [C.c_char_p, _vp, C.POINTER(_u32), _vp, C.POINTER(_u32)]),
+    "vfr_read_con": (_i, [C.c_char_p, _vp, C.POINTER(_u32), C.POINTER(_u32)]),
+    "vfr_read_extf": (_i, [C.c_char_p, _vp, C.POINTER(_u32)]),
+    "vfr_read_lmt": (_i, [C.c_char_p, _vp]),
+    "vfr_read_tf": (_i, [C.c_char_p, _vp]),
+    "vfr_write_off": (_i, [C.c_char_p, _vp, _u32, _vp, _u32]),
+    "vfr_write_con": (_i, [C.c_char_p, _vp, _u32, _u32]),
+    "vfr_write_extf": (_i, [C.c_char_p, _vp, _u32]),
+    "vfr_write_lmt": (_i, [C.c_char_p, _vp]),
+    "vfr_write_tf": (_i, [C.c_char_p, _vp]),
+    "vfr_write_ppm": (_i, [C.c_char_p, _vp, _u32, _u32]),
+    "vfr_read_psi_source": (_i, [C.c_char_p, _vp]),
+}
+
+_LIB = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load the library (once).  Raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C vfray_b200` "
+                          "or __graft_entry__.build()")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def ptr(a) -> C.c_void_p | None:
+    """Pointer of a C-contiguous numpy array or a torch tensor (None -> NULL)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("array must be C-contiguous")
+        return C.c_void_p(a.ctypes.data)
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return C.c_void_p(a.data_ptr())
+    raise TypeError(f"cannot take a pointer of {type(a)}")
+
+
+def check(rc: int, ctx=None, what: str = "") -> None:
+    if rc == VFR_OK:
+        return
+    lib = load()
+    msg = lib.vfr_status_string(rc).decode()
+    if ctx is not None:
+        detail = lib.vfr_last_error(ctx).decode()
+        if detail:
+            msg += f": {detail}"
+    raise VfrError(rc, f"{what}: {msg}" if what else msg)
