@@ -48,6 +48,12 @@ extern "C" {
 #define VFR_DEV_QUEUE 8u      /* a bounded work-queue wait gave up */
 #define VFR_DEV_OVERFLOW 16u  /* an entry list exceeded its capacity */
 
+/* Options (vfr_set_option). */
+#define VFR_OPT_STEP_CAP 1        /* per-ray tet-walk cap; 0 = 4*nT + 64 (default) */
+#define VFR_OPT_QUEUE_CHUNK 2     /* rays a warp takes from the work queue at a time (32) */
+#define VFR_OPT_BLOCKS_PER_SM 3   /* traversal CTAs per SM; 0 = occupancy maximum */
+#define VFR_OPT_PROFILE 4         /* 1: record per-stage CUDA events of every view */
+
 /* Render modes. */
 #define VFR_MODE_REF 0        /* reference semantics: last visible face wins each pixel */
 #define VFR_MODE_COMPOSITED 1 /* depth-ordered entry lists; segments composited */
@@ -78,6 +84,12 @@ VFR_API const char* vfr_status_string(int status);
 /* Use a caller-owned cudaStream_t (NULL: the context's own stream). */
 VFR_API int vfr_set_stream(vfr_ctx* ctx, void* stream);
 VFR_API int vfr_synchronize(vfr_ctx* ctx);
+/* Set a VFR_OPT_* option (negative values are invalid). */
+VFR_API int vfr_set_option(vfr_ctx* ctx, int option, int64_t value);
+/* With VFR_OPT_PROFILE on: per-view device times in ms of stage (a), (b)
+ * and (c) of the views enqueued since the last call, 3 floats per view, in
+ * order (waits for them); *count = views returned (at most cap). */
+VFR_API int vfr_profile_read(vfr_ctx* ctx, float* ms3, int cap, int* count);
 
 /* ---- tables (vfRay.cu:266-285 uploads the TF and the psi cudaArray) ---- */
 

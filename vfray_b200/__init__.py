@@ -16,7 +16,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (MODE_COMPOSITED, MODE_REF, RenderStats, VfrError, check, load, ptr,
+from ._lib import (MODE_COMPOSITED, MODE_REF, OPT_BLOCKS_PER_SM, OPT_PROFILE,
+                   OPT_QUEUE_CHUNK, OPT_STEP_CAP, RenderStats, VfrError, check, load, ptr,
                    VFR_DEV_ABANDON, VFR_DEV_OVERFLOW, VFR_DEV_QUEUE, VFR_DEV_RANGE,
                    VFR_DEV_STEP_CAP)
 
@@ -230,6 +231,18 @@ class Renderer:
     def synchronize(self):
         self._check(self.lib.vfr_synchronize(self.h), "vfr_synchronize")
 
+    def set_option(self, option: int, value: int):
+        self._check(self.lib.vfr_set_option(self.h, option, int(value)), "vfr_set_option")
+
+    def profile_read(self, cap: int = 4096) -> np.ndarray:
+        """Per-view device ms of stages (a), (b), (c) since the last read
+        (needs set_option(OPT_PROFILE, 1))."""
+        out = np.empty((cap, 3), np.float32)
+        n = C.c_int()
+        self._check(self.lib.vfr_profile_read(self.h, ptr(out), cap, C.byref(n)),
+                    "vfr_profile_read")
+        return out[: n.value].copy()
+
     def upload_tables(self, tf, psi=None):
         tf = _f32(tf, (256, 4))
         psi = None if psi is None else _f32(psi, (512, 512))
@@ -293,6 +306,17 @@ class Renderer:
         self._check(self.lib.vfr_render(self.h, mesh_id, ptr(m), W, H, mode, ptr(rgb), ptr(fa),
                                         ptr(st), C.byref(stats)), "vfr_render")
         return dict(rgb8=rgb, rgba=fa, steps=st, stats=stats.as_dict())
+
+    def render_into_host(self, mesh_id: int, W: int, H: int, rgb8: np.ndarray, mv=None,
+                         mode: int = MODE_REF):
+        """The drop-in host call: RGB8 written into the caller's (ideally
+        pinned) buffer; returns the stats."""
+        assert rgb8.dtype == np.uint8 and rgb8.flags.c_contiguous and rgb8.size == W * H * 3
+        m = None if mv is None else _f32(mv, (16,))
+        stats = RenderStats()
+        self._check(self.lib.vfr_render(self.h, mesh_id, ptr(m), W, H, mode, ptr(rgb8), None,
+                                        None, C.byref(stats)), "vfr_render")
+        return stats.as_dict()
 
     def render_device(self, mesh_id: int, W: int, H: int, mv=None, mode: int = MODE_REF,
                       rgb8=None, rgba=None, steps=None, writer=None):

@@ -31,6 +31,11 @@ VFR_DEV_RANGE = 4
 VFR_DEV_QUEUE = 8
 VFR_DEV_OVERFLOW = 16
 
+OPT_STEP_CAP = 1
+OPT_QUEUE_CHUNK = 2
+OPT_BLOCKS_PER_SM = 3
+OPT_PROFILE = 4
+
 MODE_REF = 0
 MODE_COMPOSITED = 1
 
@@ -64,6 +69,8 @@ SIGNATURES = {
     "vfr_status_string": (C.c_char_p, [_i]),
     "vfr_set_stream": (_i, [_vp, _vp]),
     "vfr_synchronize": (_i, [_vp]),
+    "vfr_set_option": (_i, [_vp, _i, C.c_int64]),
+    "vfr_profile_read": (_i, [_vp, _vp, _i, C.POINTER(_i)]),
     "vfr_tables_upload": (_i, [_vp, _vp, _vp]),
     "vfr_mesh_upload": (_i, [_vp, _vp, _u32, _vp, _vp, _u32, _vp, _u32, _f, _f, _f,
                              C.POINTER(_i)]),

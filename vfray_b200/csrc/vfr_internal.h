@@ -57,7 +57,13 @@ struct View {
 };
 
 struct Tuning {
-  uint32_t chunk = 32;  // rays per warp fetch from the ray queue
+  uint32_t chunk = 32;        // rays per warp fetch from the ray queue
+  uint32_t blocks_per_sm = 0; // traversal CTAs per SM (0: occupancy maximum)
+};
+
+// Four events bracketing the stages of one view (profiling).
+struct StageEvents {
+  cudaEvent_t e[4] = {};
 };
 
 struct Ctx {
@@ -76,6 +82,11 @@ struct Ctx {
   uint32_t step_cap = 0;
   size_t ent_cap_hint = 0;
   Tuning tune;
+  bool profile = false;
+  std::vector<StageEvents> prof_pool;  // recycled events
+  std::vector<StageEvents> prof_live;  // recorded, not yet read
+  StageEvents* prof_cur = nullptr;
+  void prof_mark(int k);
 
   ~Ctx() {
     meshes.clear();
@@ -84,6 +95,10 @@ struct Ctx {
     if (h_ctr) cudaFreeHost(h_ctr);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
+    for (auto* v : {&prof_pool, &prof_live})
+      for (auto& s : *v)
+        for (auto& e : s.e)
+          if (e) cudaEventDestroy(e);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
 

@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(256) raster_kernel(
     const EntryEdges E = entry_edges(v0, v1, v2);
     const float4 p0 = planes[2 * (size_t)e], p1 = planes[2 * (size_t)e + 1];
     const uint32_t xe = min(bz, W - 1), ye = min(bw, H - 1);
+    if (bx > xe || by > ye) continue;  // box entirely outside the image
     for (uint32_t px = bx + lane; px <= xe; px += 32) {
       const float ox = obj_coord(px, W);
       for (uint32_t py = by; py <= ye; ++py) {

@@ -195,7 +195,23 @@ int Ctx::enqueue_traverse(View& v, uint8_t* rgb8, float4* rgba, uint32_t* steps)
   return cuda(cudaGetLastError(), "stage (c) launch");
 }
 
+void Ctx::prof_mark(int k) {
+  if (!profile) return;
+  if (k == 0) {
+    StageEvents s;
+    if (!prof_pool.empty()) {
+      s = prof_pool.back();
+      prof_pool.pop_back();
+    } else {
+      for (auto& e : s.e) cudaEventCreate(&e);
+    }
+    prof_live.push_back(s);
+  }
+  cudaEventRecord(prof_live.back().e[k], stream);
+}
+
 int Ctx::traverse_blocks_per_sm(int mode) {
+  if (tune.blocks_per_sm) return (int)tune.blocks_per_sm;
   int& cached = occ[mode ? 1 : 0];
   if (!cached) {
     int n = 0;
@@ -286,6 +302,39 @@ int vfr_set_stream(vfr_ctx* c, void* stream) {
 int vfr_synchronize(vfr_ctx* c) {
   CTX_OR_FAIL(c);
   return C.cuda(cudaStreamSynchronize(C.stream), "synchronize");
+}
+
+int vfr_set_option(vfr_ctx* c, int option, int64_t value) {
+  CTX_OR_FAIL(c);
+  if (value < 0 || value > 0x7fffffff) return C.fail(VFR_ERR_INVALID, "option value out of range");
+  switch (option) {
+    case VFR_OPT_STEP_CAP: C.step_cap = (uint32_t)value; return VFR_OK;
+    case VFR_OPT_QUEUE_CHUNK:
+      if (value < 1) return C.fail(VFR_ERR_INVALID, "queue chunk must be >= 1");
+      C.tune.chunk = (uint32_t)value;
+      return VFR_OK;
+    case VFR_OPT_BLOCKS_PER_SM: C.tune.blocks_per_sm = (uint32_t)value; return VFR_OK;
+    case VFR_OPT_PROFILE: C.profile = value != 0; return VFR_OK;
+    default: return C.fail(VFR_ERR_INVALID, "unknown option");
+  }
+}
+
+int vfr_profile_read(vfr_ctx* c, float* ms3, int cap, int* count) {
+  CTX_OR_FAIL(c);
+  if (!count || (cap > 0 && !ms3)) return C.fail(VFR_ERR_INVALID, "bad profile buffer");
+  int n = 0;
+  for (auto& s : C.prof_live) {
+    int rc = C.cuda(cudaEventSynchronize(s.e[3]), "profile event");
+    if (rc) return rc;
+    if (n < cap) {
+      for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&ms3[3 * n + k], s.e[k], s.e[k + 1]);
+      ++n;
+    }
+    C.prof_pool.push_back(s);
+  }
+  C.prof_live.clear();
+  *count = n;
+  return VFR_OK;
 }
 
 int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
@@ -502,12 +551,16 @@ static int render_common(Ctx& C, int id, const float* mv16, uint32_t W, uint32_t
     C.view.ent_cap = want;
   }
   if (timed) cudaEventRecord(C.ev[0], C.stream);
+  C.prof_mark(0);
   int rc = C.enqueue_visible(*m, mv16, C.view);
   if (timed) cudaEventRecord(C.ev[1], C.stream);
+  C.prof_mark(1);
   if (!rc) rc = C.enqueue_project(C.view, W, H, mode);
   if (timed) cudaEventRecord(C.ev[2], C.stream);
+  C.prof_mark(2);
   if (!rc) rc = C.enqueue_traverse(C.view, rgb8, rgba, steps);
   if (timed) cudaEventRecord(C.ev[3], C.stream);
+  C.prof_mark(3);
   if (!rc && writer_dev && mode == VFR_MODE_REF)
     rc = C.cuda(cudaMemcpyAsync(writer_dev, C.view.winner.p, sizeof(int32_t) * (size_t)W * H,
                                 cudaMemcpyDeviceToDevice, C.stream),
