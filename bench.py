@@ -140,7 +140,8 @@ class Clocks:
             return None
         sm = np.array([r[0] for r in rows])
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[2][k]})
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[2][k].strip().lower() == "active"})
         loaded = sm[sm >= 0.5 * sm.max()] if sm.max() > 0 else sm
         return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": float(rows[0][1]),
                 "reasons": reasons, "samples": len(rows)}
@@ -394,6 +395,10 @@ def run_reference(args, rank):
                     "d2h_bytes_per_step": 0}}
 
 
+def _json(o):
+    return json.dumps(o, default=lambda x: x.item() if hasattr(x, "item") else str(x))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -402,7 +407,7 @@ def main():
     if args.impl == "reference":
         out = run_reference(args, rank)
         if out is not None:
-            print(json.dumps(out))
+            print(_json(out))
         return
     if world > 1:
         import datetime
@@ -427,7 +432,7 @@ def main():
         out["cpu_baseline"] = cpu_baseline(wl, args.cpu_seconds)
     if dist:
         dist.destroy_process_group()
-    print(json.dumps(out))
+    print(_json(out))
 
 
 if __name__ == "__main__":

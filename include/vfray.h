@@ -53,6 +53,8 @@ extern "C" {
 #define VFR_OPT_QUEUE_CHUNK 2     /* rays a warp takes from the work queue at a time (32) */
 #define VFR_OPT_BLOCKS_PER_SM 3   /* traversal CTAs per SM; 0 = occupancy maximum */
 #define VFR_OPT_PROFILE 4         /* 1: record per-stage CUDA events of every view */
+#define VFR_OPT_TRAVERSE_VARIANT 5 /* traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM */
+#define VFR_OPT_REFILL 6          /* refill a warp's idle lanes once >= this many are idle (1) */
 
 /* Render modes. */
 #define VFR_MODE_REF 0        /* reference semantics: last visible face wins each pixel */

@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from ._lib import (MODE_COMPOSITED, MODE_REF, OPT_BLOCKS_PER_SM, OPT_PROFILE,
-                   OPT_QUEUE_CHUNK, OPT_STEP_CAP, RenderStats, VfrError, check, load, ptr,
+                   OPT_QUEUE_CHUNK, OPT_REFILL, OPT_STEP_CAP, OPT_TRAVERSE_VARIANT, RenderStats, VfrError, check, load, ptr,
                    VFR_DEV_ABANDON, VFR_DEV_OVERFLOW, VFR_DEV_QUEUE, VFR_DEV_RANGE,
                    VFR_DEV_STEP_CAP)
 

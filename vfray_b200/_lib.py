@@ -35,6 +35,8 @@ OPT_STEP_CAP = 1
 OPT_QUEUE_CHUNK = 2
 OPT_BLOCKS_PER_SM = 3
 OPT_PROFILE = 4
+OPT_TRAVERSE_VARIANT = 5
+OPT_REFILL = 6
 
 MODE_REF = 0
 MODE_COMPOSITED = 1

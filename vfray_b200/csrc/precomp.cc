@@ -18,7 +18,7 @@
 #include <thread>
 #include <vector>
 
-#include "../../include/vfray.h"
+#include "vfray.h"
 
 namespace {
 

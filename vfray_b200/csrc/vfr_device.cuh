@@ -15,11 +15,30 @@ namespace vfr {
 
 constexpr double kRDelta = 1e-12;  // vfRayKernelCPU.h:28 (a double)
 
-// Packed tet record: 4 vertex ids + 4 neighbour ids (conTet row), 32 bytes.
-struct __align__(16) TetRec {
-  uint4 v;
+// Walk record of a tet, 32 bytes: the 4 neighbour ids (the conTet row, self
+// = boundary) and, per face f, one packed word q[f] describing the neighbour
+// n across f: bits 0-26 the id of n's vertex opposite the shared face (the
+// only vertex of n a ray entering n through that face does not already
+// hold), bits 27-28 the face of n it is entered through (the first k with
+// conTet[4n+k] == t, as vfRayKernelCPU.cc:361-364 finds it), bits 29-31 how
+// n orders the shared face's vertices: a permutation code 0-5 (perm_code), 6 if
+// the ids do not match (the walk then reloads n's vertices), 7 for a
+// boundary face.  The walk reads only these records; vertex ids of a tet
+// come from the plain tet array (uint4 per tet) when a ray starts.
+struct __align__(16) WalkRec {
   uint4 n;
+  uint4 q;
 };
+
+// perm_code(k) packs, for j = 0..2, which vertex of the exit face (0, 1, 2
+// in the current tet's order) sits at slot (fn + j) of the next tet, 2 bits
+// each, for the 6 permutations k = (012, 021, 102, 120, 201, 210).
+__host__ __device__ __forceinline__ uint32_t perm_code(uint32_t k) {
+  // 6-bit fields: 0b100100, 0b011000, 0b100001, 0b001001, 0b010010, 0b000110
+  constexpr unsigned long long kLut = 0x24ull | 0x18ull << 6 | 0x21ull << 12 | 0x09ull << 18 |
+                                      0x12ull << 24 | 0x06ull << 30;
+  return (uint32_t)(kLut >> (6 * k)) & 63u;
+}
 
 struct Plane {
   float zx, zy, zz, sx, sy, sz;
@@ -34,10 +53,11 @@ __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
-// ABS(n) ((n) < 0 ? -(n) : (n)) compared against the double RDELTA
+// ABS(n) ((n) < 0 ? -(n) : (n)) compared against the double RDELTA: for a
+// float a, (double)a < 1e-12 exactly when a <= 0x2b8cbccc (9.9999996e-13, the
+// largest float below 1e-12), so the comparison needs no conversion.
 __device__ __forceinline__ bool below_rdelta(float v) {
-  float a = v < 0.0f ? -v : v;
-  return (double)a < kRDelta;
+  return fabsf(v) <= __uint_as_float(0x2b8cbcccu);
 }
 
 __device__ __forceinline__ uint32_t sel4(uint4 v, uint32_t i) {
@@ -45,14 +65,6 @@ __device__ __forceinline__ uint32_t sel4(uint4 v, uint32_t i) {
   r = (i == 1) ? v.y : r;
   r = (i == 2) ? v.z : r;
   r = (i == 3) ? v.w : r;
-  return r;
-}
-
-__device__ __forceinline__ float4 sel4(const float4 (&v)[4], uint32_t i) {
-  float4 r = v[0];
-  if (i == 1) r = v[1];
-  if (i == 2) r = v[2];
-  if (i == 3) r = v[3];
   return r;
 }
 
@@ -132,34 +144,6 @@ __device__ __forceinline__ bool entry_inside(const EntryEdges& E, float ox, floa
   float cy = fsub(fmul(E.e1x, py), fmul(E.e1y, px));
   float cz = fsub(fmul(px, E.e2y), fmul(py, E.e2x));
   return (cy >= 0.0f) && (cz >= 0.0f) && (fadd(cy, cz) <= E.cx);
-}
-
-// Exit-face search among the 3 faces other than the entry face
-// (vfRayKernelCPU.cc:312-350): 2-D edge functions with +RDELTA slack on the
-// sum, faces with |cross| < RDELTA skipped.  Returns the entry face itself
-// when no face qualifies (the reference's "anomaly" end of the ray).
-__device__ __forceinline__ uint32_t find_exit(const float4 (&fv)[4], uint32_t entry, float ox,
-                                              float oy) {
-#pragma unroll
-  for (uint32_t i = 1; i < 4; ++i) {
-    const uint32_t id = (entry + i) & 3u;
-    const float4 a = sel4(fv, id), b = sel4(fv, (id + 1) & 3u), c = sel4(fv, (id + 2) & 3u);
-    float v1x = fsub(b.x, a.x), v1y = fsub(b.y, a.y);
-    float v2x = fsub(c.x, a.x), v2y = fsub(c.y, a.y);
-    float cr = fsub(fmul(v1x, v2y), fmul(v1y, v2x));
-    if (below_rdelta(cr)) continue;
-    if (cr < 0.0f) {
-      float tx = v1x, ty = v1y;
-      v1x = v2x; v1y = v2y; v2x = tx; v2y = ty;
-      cr = -cr;
-    }
-    const float v0x = fsub(ox, a.x), v0y = fsub(oy, a.y);
-    const float c1 = fsub(fmul(v1x, v0y), fmul(v1y, v0x));
-    const float c2 = fsub(fmul(v0x, v2y), fmul(v0y, v2x));
-    if ((c1 >= 0.0f) && (c2 >= 0.0f) && ((double)fadd(c1, c2) <= dadd((double)cr, kRDelta)))
-      return id;
-  }
-  return entry;
 }
 
 // Orderable encoding of floats for atomicMin/atomicMax on unsigned ints.

@@ -10,4 +10,9 @@ namespace vfr {
 bool validate_mesh(const uint32_t* tet4, const uint32_t* con4, uint32_t nV, uint32_t nT,
                    const uint32_t* extf2, uint32_t nExt, std::string& why);
 
+// Walk records: per tet 8 words (4 neighbour ids, 4 packed opposite-vertex
+// words); nV must be below 2^27 (vfr_validate.cc).
+bool build_walk(const uint32_t* tet4, const uint32_t* con4, uint32_t nV, uint32_t nT,
+                uint32_t* walk8, std::string& why);
+
 }  // namespace vfr

@@ -28,12 +28,14 @@ struct Buf {
 struct Mesh {
   uint32_t nV = 0, nT = 0, nExt = 0;
   float maxEdge = 0, maxZ = 0, minZ = 0;
-  TetRec* rec = nullptr;
+  uint4* tet = nullptr;     // vertex ids per tet (the reference's tetList)
+  WalkRec* walk = nullptr;  // neighbour + opposite-vertex words per tet
   float4* vert = nullptr;
   uint2* extf = nullptr;
   size_t bytes = 0;
   ~Mesh() {
-    if (rec) cudaFree(rec);
+    if (tet) cudaFree(tet);
+    if (walk) cudaFree(walk);
     if (vert) cudaFree(vert);
     if (extf) cudaFree(extf);
   }
@@ -59,6 +61,8 @@ struct View {
 struct Tuning {
   uint32_t chunk = 32;        // rays per warp fetch from the ray queue
   uint32_t blocks_per_sm = 0; // traversal CTAs per SM (0: occupancy maximum)
+  uint32_t refill = 1;        // refill idle lanes once this many of a warp's are idle
+  uint32_t variant = 0;       // traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM
 };
 
 // Four events bracketing the stages of one view (profiling).
@@ -73,12 +77,13 @@ struct Ctx {
   std::string err;
   float4* d_tf = nullptr;
   float* d_psi = nullptr;
+  bool psi_one = false;  // psi[0][0] == 1.0f
   std::vector<std::unique_ptr<Mesh>> meshes;
   View view;
   Buf out_rgb8, out_rgba, out_steps;
   ViewCounters* h_ctr = nullptr;
   cudaEvent_t ev[4] = {};
-  int occ[2] = {0, 0};
+  int occ[4] = {0, 0, 0, 0};
   uint32_t step_cap = 0;
   size_t ent_cap_hint = 0;
   Tuning tune;
@@ -110,6 +115,7 @@ struct Ctx {
   int enqueue_project(View& v, uint32_t W, uint32_t H, int mode);
   int enqueue_traverse(View& v, uint8_t* rgb8, float4* rgba, uint32_t* steps);
   int traverse_blocks_per_sm(int mode);
+  const void* traverse_fn(int mode, uint32_t variant);
   int read_counters(View& v, ViewCounters& out);
   int check_status(const ViewCounters& c);
 };

@@ -19,7 +19,8 @@ struct __align__(16) ViewCounters {
 };
 
 struct TraverseParams {
-  const TetRec* rec;
+  const uint4* tet;
+  const WalkRec* walk;
   const float4* vert;
   const uint2* extf;
   const float4* planes;   // 2 float4 per ext face: (zx zy zz sx) (sy sz - -)
@@ -37,8 +38,10 @@ struct TraverseParams {
   float maxEdge;          // used when use_view_maxedge == 0
   int use_view_maxedge;
   uint32_t step_cap;
-  uint32_t chunk;         // rays per warp fetch
+  uint32_t chunk;         // rays per warp fetch (unused by the refill kernel)
   uint32_t ent_cap;       // composited: capacity of ent
+  uint32_t refill;        // refill a warp's idle lanes once at least this many are idle
+  uint32_t psi_one;       // psi table[0][0] == 1.0f (enables the zero-extinction shortcut)
 };
 
 // ---------------------------------------------------------------- view set-up
@@ -116,11 +119,11 @@ __global__ void view_normalize_kernel(float4* __restrict__ v, uint32_t nV, const
 }
 
 // buildLmt's maxEdgeLength (vfRayPreComp.cc:810-836) over the view's vertices.
-__global__ void view_maxedge_kernel(const TetRec* __restrict__ rec, const float4* __restrict__ v,
+__global__ void view_maxedge_kernel(const uint4* __restrict__ tet, const float4* __restrict__ v,
                                     uint32_t nT, ViewCounters* ctr) {
   float best = 0.0f;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nT; t += gridDim.x * blockDim.x) {
-    const uint4 id = rec[t].v;
+    const uint4 id = tet[t];
     const float4 p[4] = {v[id.x], v[id.y], v[id.z], v[id.w]};
     const int E[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
 #pragma unroll
@@ -140,7 +143,7 @@ __global__ void view_maxedge_kernel(const TetRec* __restrict__ rec, const float4
 // findVisibleFaces (vfRayKernelCPU.cc:51-132), one thread per external face;
 // writes the face planes and the per-block count of visible faces.
 __global__ void __launch_bounds__(1024) visible_kernel(const float4* __restrict__ vert,
-                                                       const TetRec* __restrict__ rec,
+                                                       const uint4* __restrict__ tet,
                                                        const uint2* __restrict__ extf,
                                                        uint32_t nExt, float4* __restrict__ planes,
                                                        uint32_t* __restrict__ blk_cnt) {
@@ -148,7 +151,7 @@ __global__ void __launch_bounds__(1024) visible_kernel(const float4* __restrict_
   int vis = 0;
   if (e < nExt) {
     const uint2 tf = extf[e];
-    const uint4 id = rec[tf.x].v;
+    const uint4 id = tet[tf.x];
     const float4 v0 = vert[sel4(id, tf.y & 3u)];
     const float4 v1 = vert[sel4(id, (tf.y + 1) & 3u)];
     const float4 v2 = vert[sel4(id, (tf.y + 2) & 3u)];
@@ -218,7 +221,7 @@ __global__ void __launch_bounds__(1024) compact_kernel(const float4* __restrict_
 // are clipped (the reference would write past its buffer there).
 template <bool kCount, bool kFill>
 __global__ void __launch_bounds__(256) raster_kernel(
-    const float4* __restrict__ vert, const TetRec* __restrict__ rec, const uint2* __restrict__ extf,
+    const float4* __restrict__ vert, const uint4* __restrict__ tet, const uint2* __restrict__ extf,
     const float4* __restrict__ planes, const uint32_t* __restrict__ vis_ext, ViewCounters* ctr,
     uint32_t W, uint32_t H, uint4* __restrict__ bbox, int32_t* __restrict__ winner,
     uint32_t* __restrict__ ent_cnt, const uint32_t* __restrict__ ent_off,
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(256) raster_kernel(
   for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nvis; i += nwarps) {
     const uint32_t e = vis_ext[i];
     const uint2 tf = extf[e];
-    const uint4 id = rec[tf.x].v;
+    const uint4 id = tet[tf.x];
     const float4 v0 = vert[sel4(id, tf.y & 3u)];
     const float4 v1 = vert[sel4(id, (tf.y + 1) & 3u)];
     const float4 v2 = vert[sel4(id, (tf.y + 2) & 3u)];
@@ -350,194 +353,6 @@ __global__ void __launch_bounds__(1024) scan_add_kernel(uint32_t* __restrict__ o
     *total = s_base + sums[blockIdx.x];
 }
 
-// ------------------------------------------------------------------ stage (c)
-
-struct RayAcc {
-  float r, g, b, trans;
-};
-
-// One ray segment (vfRayKernelCPU.cc:276-542).  The current tet's 4 vertex
-// ids and neighbour ids come from one 32-byte record; its 4 vertices stay in
-// registers, so a step loads the next record and only the vertices it does
-// not already hold (normally one).  Returns 0, or VFR_DEV_* bits.
-__device__ __forceinline__ uint32_t walk_segment(const TraverseParams& P, const float4* s_tf,
-                                                 float maxEdge, float ox, float oy, uint32_t t,
-                                                 uint32_t f, float zp, float sp, RayAcc& acc,
-                                                 uint32_t& iters, float& lastZ) {
-  TetRec R = P.rec[t];
-  float4 fv[4];
-  fv[0] = P.vert[R.v.x];
-  fv[1] = P.vert[R.v.y];
-  fv[2] = P.vert[R.v.z];
-  fv[3] = P.vert[R.v.w];
-  float4 cb = s_tf[(uint32_t)fmul(255.0f, sp)];
-  lastZ = zp;
-  for (;;) {
-    if (++iters > P.step_cap) return 2u;  // VFR_DEV_STEP_CAP
-    const uint32_t ex = find_exit(fv, f, ox, oy);
-    if (ex == f) return 0u;  // :353
-    const uint32_t tn = sel4(R.n, ex);
-    const bool leaving = (tn == t);
-    TetRec N = R;
-    uint32_t fn = f;
-    if (!leaving) {
-      if (tn >= P.nT) return 4u;  // VFR_DEV_RANGE
-      N = P.rec[tn];
-      fn = (N.n.x == t) ? 0u : (N.n.y == t) ? 1u : (N.n.z == t) ? 2u : (N.n.w == t) ? 3u : 4u;
-      if (fn == 4u) return 1u;  // :365 VFR_DEV_ABANDON
-    }
-    Plane nf;
-    face_plane(sel4(fv, ex), sel4(fv, (ex + 1) & 3u), sel4(fv, (ex + 2) & 3u), nf);
-    const float zn = plane_eval(ox, oy, nf.zx, nf.zy, nf.zz);
-    const float sn = plane_eval(ox, oy, nf.sx, nf.sy, nf.sz);
-    float dz = fsub(zp, zn);
-    dz = dz < 0.0f ? -dz : dz;
-    dz = ((double)dz < kRDelta) ? 0.0f : dz;
-    if ((sn < 0.0f) || (sn > 1.0f)) return 0u;  // :446
-    dz = fdiv(dz, maxEdge);
-    const float4 cf = s_tf[(uint32_t)fmul(255.0f, sn)];
-    const float taux = fmul(cf.w, dz), tauy = fmul(cb.w, dz);
-    const float zeta = (float)exp(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)));
-    const float gx = (float)ddiv((double)taux, dadd(1.0, (double)taux));
-    const float gy = (float)ddiv((double)tauy, dadd(1.0, (double)tauy));
-    const float tcx = (float)dadd((double)gx, 0.5 / 512), tcy = (float)dadd((double)gy, 0.5 / 512);
-    if ((tcx < 0.0f) || (tcx > 1.0f) || (tcy < 0.0f) || (tcy > 1.0f)) return 0u;  // :468
-    const uint32_t pi = min((uint32_t)fmul(tcx, 512.0f), 511u);
-    const uint32_t pj = min((uint32_t)fmul(tcy, 512.0f), 511u);
-    const double psi = (double)__ldg(P.psi + pi * 512u + pj);
-    const double dzeta = (double)zeta;
-    const double a = dsub(1.0, psi), b = dsub(psi, dzeta);
-    const float fr = (float)dadd(dmul((double)cf.x, a), dmul((double)cb.x, b));
-    const float fg = (float)dadd(dmul((double)cf.y, a), dmul((double)cb.y, b));
-    const float fb = (float)dadd(dmul((double)cf.z, a), dmul((double)cb.z, b));
-    const float fw = (float)dsub(1.0, dzeta);
-    const double keep = dsub(1.0, (double)fw);
-    acc.r = (float)dadd((double)fr, dmul(keep, (double)acc.r));
-    acc.g = (float)dadd((double)fg, dmul(keep, (double)acc.g));
-    acc.b = (float)dadd((double)fb, dmul(keep, (double)acc.b));
-    acc.trans = fmul(acc.trans, zeta);
-    lastZ = zn;
-    cb = cf;
-    if (leaving) return 0u;  // :535
-    // advance: keep the vertices shared with the next tet, load the rest
-    float4 nv[4];
-    const uint32_t ids[4] = {N.v.x, N.v.y, N.v.z, N.v.w};
-    const uint32_t old[4] = {R.v.x, R.v.y, R.v.z, R.v.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const uint32_t q = ids[k];
-      const bool h0 = q == old[0], h1 = q == old[1], h2 = q == old[2], h3 = q == old[3];
-      if (h0 | h1 | h2 | h3) {
-        float4 r = fv[0];
-        if (h1) r = fv[1];
-        if (h2) r = fv[2];
-        if (h3) r = fv[3];
-        nv[k] = r;
-      } else {
-        nv[k] = P.vert[q];
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) fv[k] = nv[k];
-    R = N;
-    t = tn;
-    f = fn;
-    zp = zn;
-    sp = sn;
-  }
-}
-
-__device__ __forceinline__ void write_pixel(const TraverseParams& P, uint32_t p, const RayAcc& acc,
-                                            uint32_t iters) {
-  float c[3] = {acc.r, acc.g, acc.b};
-#pragma unroll
-  for (int k = 0; k < 3; ++k) c[k] = (c[k] > 1.0f) ? 1.0f : c[k];  // :546-548
-  if (P.rgb8) {
-    uint8_t* o = P.rgb8 + 3 * (size_t)p;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o[k] = (uint8_t)__float2int_rz(fmul(255.0f, c[k]));  // :550-552
-  }
-  if (P.rgba) P.rgba[p] = make_float4(c[0], c[1], c[2], fsub(1.0f, acc.trans));
-  if (P.steps) P.steps[p] = iters;
-}
-
-// Stage (c): persistent warps pull `chunk` rays at a time from the view's
-// ray list; one lane per ray.  kMode 0: the reference's winner face per
-// pixel; kMode 1: the depth-sorted entry list of the pixel, segments
-// composited in order.
-template <int kMode>
-__global__ void __launch_bounds__(256) traverse_kernel(TraverseParams P) {
-  __shared__ float4 s_tf[256];
-  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tf[i] = P.tf[i];
-  __syncthreads();
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t nrays = P.ctr->nrays;
-  const float maxEdge = P.use_view_maxedge ? __uint_as_float(P.ctr->maxedge_bits) : P.maxEdge;
-  unsigned long long my_steps = 0;
-  uint32_t status = 0;
-  for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&P.ctr->queue, P.chunk);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= nrays) break;
-    const uint32_t end = min(base + P.chunk, nrays);
-    for (uint32_t r = base + lane; r < end; r += 32) {
-      const uint32_t p = P.rays[r];
-      const uint32_t x = p % P.W, y = p / P.W;
-      const float ox = obj_coord(x, P.W), oy = obj_coord(y, P.H);
-      RayAcc acc = {0.0f, 0.0f, 0.0f, 1.0f};
-      uint32_t iters = 0, st = 0;
-      float lastZ;
-      if (kMode == 0) {
-        const uint32_t e = (uint32_t)P.winner[p];
-        const uint2 tf = P.extf[e];
-        const float4 p0 = P.planes[2 * (size_t)e], p1 = P.planes[2 * (size_t)e + 1];
-        const float zp = plane_eval(ox, oy, p0.x, p0.y, p0.z);
-        const float sp = plane_eval(ox, oy, p0.w, p1.x, p1.y);
-        st = walk_segment(P, s_tf, maxEdge, ox, oy, tf.x, tf.y, zp, sp, acc, iters, lastZ);
-      } else {
-        // entries sorted by depth (descending), ties by ext index (descending)
-        const uint32_t a = P.ent_off[p], n = P.ent_off[p + 1] - a;
-        if (P.ent_off[p + 1] > P.ent_cap) {  // entry lists overflowed: caller renders again
-          status |= 16u;  // VFR_DEV_OVERFLOW
-          continue;
-        }
-        float exitZ = INFINITY;
-        uint32_t done_z = 0xffffffffu, done_e = 0xffffffffu;  // last taken (ordered) key
-        for (uint32_t s = 0; s < n && !st; ++s) {
-          // selection of the next entry in order: largest (z, e) below the last one
-          float bz = -INFINITY;
-          uint32_t be = 0, bzbits = 0;
-          bool found = false;
-          for (uint32_t k = 0; k < n; ++k) {
-            const uint2 q = P.ent[a + k];
-            const float z = __uint_as_float(q.x);
-            const bool below = (s == 0) || (z < __uint_as_float(done_z)) ||
-                               (z == __uint_as_float(done_z) && q.y < done_e);
-            if (!below) continue;
-            if (!found || z > bz || (z == bz && q.y > be)) {
-              bz = z; be = q.y; bzbits = q.x; found = true;
-            }
-          }
-          if (!found) break;
-          done_z = bzbits; done_e = be;
-          if (bz > exitZ) continue;
-          const uint2 tf = P.extf[be];
-          const float4 p0 = P.planes[2 * (size_t)be], p1 = P.planes[2 * (size_t)be + 1];
-          const float sp = plane_eval(ox, oy, p0.w, p1.x, p1.y);
-          st = walk_segment(P, s_tf, maxEdge, ox, oy, tf.x, tf.y, bz, sp, acc, iters, lastZ);
-          exitZ = lastZ;
-        }
-      }
-      my_steps += iters;
-      if (st & 1u) { status |= st; continue; }  // abandoned: the reference writes nothing
-      status |= st;
-      write_pixel(P, p, acc, iters);
-    }
-  }
-  for (int o = 16; o; o >>= 1) my_steps += __shfl_xor_sync(0xffffffffu, my_steps, o);
-  if (lane == 0 && my_steps) atomicAdd(&P.ctr->steps, my_steps);
-  if (status) atomicOr(&P.ctr->status, status);
-}
-
 }  // namespace vfr
+
+#include "vfr_traverse.cuh"

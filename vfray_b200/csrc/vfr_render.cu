@@ -14,7 +14,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/vfray.h"
+#include "vfray.h"
 #include "vfr_kernels.cuh"
 #include "vfr_internal.h"
 
@@ -93,7 +93,7 @@ int Ctx::enqueue_visible(Mesh& m, const float* mv16, View& v) {
         make_float4(mv16[8], mv16[9], mv16[10], mv16[11]), vv, v.ctr);
     view_normalize_kernel<<<blocks, 256, 0, stream>>>(vv, m.nV, v.ctr);
     const int tb = std::max(1, std::min(num_sms * 4, (int)((m.nT + 255) / 256)));
-    view_maxedge_kernel<<<tb, 256, 0, stream>>>(m.rec, vv, m.nT, v.ctr);
+    view_maxedge_kernel<<<tb, 256, 0, stream>>>(m.tet, vv, m.nT, v.ctr);
     v.vert = vv;
     v.use_view_maxedge = 1;
   }
@@ -103,7 +103,7 @@ int Ctx::enqueue_visible(Mesh& m, const float* mv16, View& v) {
   if (!rc) rc = grow(v.vis_ext, sizeof(uint32_t) * std::max<uint32_t>(m.nExt, 1), "visible list");
   if (rc) return rc;
   if (m.nExt) {
-    visible_kernel<<<nblk, 1024, 0, stream>>>(v.vert, m.rec, m.extf, m.nExt, (float4*)v.planes.p,
+    visible_kernel<<<nblk, 1024, 0, stream>>>(v.vert, m.tet, m.extf, m.nExt, (float4*)v.planes.p,
                                              (uint32_t*)v.blk.p);
     compact_kernel<<<nblk, 1024, 0, stream>>>((const float4*)v.planes.p, m.nExt,
                                              (const uint32_t*)v.blk.p, (uint32_t*)v.vis_ext.p,
@@ -130,7 +130,7 @@ int Ctx::enqueue_project(View& v, uint32_t W, uint32_t H, int mode) {
     cudaMemsetAsync(v.winner.p, 0xff, sizeof(int32_t) * np, stream);
     if (m.nExt)
       raster_kernel<false, false><<<rb, 256, 0, stream>>>(
-          v.vert, m.rec, m.extf, planes, vis, v.ctr, W, H, (uint4*)v.bbox.p,
+          v.vert, m.tet, m.extf, planes, vis, v.ctr, W, H, (uint4*)v.bbox.p,
           (int32_t*)v.winner.p, nullptr, nullptr, nullptr, nullptr, 0);
   } else {
     const uint32_t nsb = (uint32_t)((np + 1 + 1023) / 1024);
@@ -144,7 +144,7 @@ int Ctx::enqueue_project(View& v, uint32_t W, uint32_t H, int mode) {
     cudaMemsetAsync(v.ent_cur.p, 0, sizeof(uint32_t) * np, stream);
     if (m.nExt)
       raster_kernel<true, false><<<rb, 256, 0, stream>>>(
-          v.vert, m.rec, m.extf, planes, vis, v.ctr, W, H, (uint4*)v.bbox.p, nullptr,
+          v.vert, m.tet, m.extf, planes, vis, v.ctr, W, H, (uint4*)v.bbox.p, nullptr,
           (uint32_t*)v.ent_cnt.p, nullptr, nullptr, nullptr, 0);
     scan_blocks_kernel<<<nsb, 1024, 0, stream>>>((const uint32_t*)v.ent_cnt.p, (uint32_t)(np + 1),
                                                  (uint32_t*)v.ent_off.p, (uint32_t*)v.scan.p);
@@ -152,7 +152,7 @@ int Ctx::enqueue_project(View& v, uint32_t W, uint32_t H, int mode) {
                                               (const uint32_t*)v.scan.p, &v.ctr->nentries);
     if (m.nExt)
       raster_kernel<false, true><<<rb, 256, 0, stream>>>(
-          v.vert, m.rec, m.extf, planes, vis, v.ctr, W, H, nullptr, nullptr, nullptr,
+          v.vert, m.tet, m.extf, planes, vis, v.ctr, W, H, nullptr, nullptr, nullptr,
           (const uint32_t*)v.ent_off.p, (uint32_t*)v.ent_cur.p, (uint2*)v.ent.p,
           (uint32_t)std::min<size_t>(v.ent_cap, 0xffffffffu));
   }
@@ -172,7 +172,7 @@ int Ctx::enqueue_traverse(View& v, uint8_t* rgb8, float4* rgba, uint32_t* steps)
   if (rgba) cudaMemsetAsync(rgba, 0, np * sizeof(float4), stream);
   if (steps) cudaMemsetAsync(steps, 0, np * sizeof(uint32_t), stream);
   TraverseParams P;
-  P.rec = m.rec; P.vert = v.vert; P.extf = m.extf;
+  P.tet = m.tet; P.walk = m.walk; P.vert = v.vert; P.extf = m.extf;
   P.planes = (const float4*)v.planes.p;
   P.winner = (const int32_t*)v.winner.p;
   P.rays = (const uint32_t*)v.rays.p;
@@ -186,13 +186,19 @@ int Ctx::enqueue_traverse(View& v, uint8_t* rgb8, float4* rgba, uint32_t* steps)
   P.use_view_maxedge = v.use_view_maxedge;
   P.step_cap = step_cap ? step_cap : (uint32_t)std::min<uint64_t>(4ull * m.nT + 64, 0x7fffffffull);
   P.chunk = tune.chunk;
+  P.refill = tune.refill;
+  P.psi_one = psi_one ? 1u : 0u;
   P.ent_cap = (uint32_t)std::min<size_t>(v.ent_cap, 0xffffffffu);
   const int blocks = num_sms * traverse_blocks_per_sm(v.mode);
-  if (v.mode == VFR_MODE_REF)
-    traverse_kernel<0><<<blocks, 256, 0, stream>>>(P);
-  else
-    traverse_kernel<1><<<blocks, 256, 0, stream>>>(P);
-  return cuda(cudaGetLastError(), "stage (c) launch");
+  const void* fn = traverse_fn(v.mode, tune.variant);
+  void* args[] = {&P};
+  return cuda(cudaLaunchKernel(fn, dim3(blocks), dim3(256), args, 0, stream), "stage (c) launch");
+}
+
+const void* Ctx::traverse_fn(int mode, uint32_t variant) {
+  if (mode == VFR_MODE_REF)
+    return variant ? (const void*)traverse_kernel<0, 3> : (const void*)traverse_kernel<0, 2>;
+  return variant ? (const void*)traverse_kernel<1, 3> : (const void*)traverse_kernel<1, 2>;
 }
 
 void Ctx::prof_mark(int k) {
@@ -212,13 +218,10 @@ void Ctx::prof_mark(int k) {
 
 int Ctx::traverse_blocks_per_sm(int mode) {
   if (tune.blocks_per_sm) return (int)tune.blocks_per_sm;
-  int& cached = occ[mode ? 1 : 0];
+  int& cached = occ[(mode ? 2 : 0) + (tune.variant ? 1 : 0)];
   if (!cached) {
     int n = 0;
-    if (mode == VFR_MODE_REF)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_kernel<0>, 256, 0);
-    else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_kernel<1>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_fn(mode, tune.variant), 256, 0);
     cached = std::max(1, n);
   }
   return cached;
@@ -315,6 +318,14 @@ int vfr_set_option(vfr_ctx* c, int option, int64_t value) {
       return VFR_OK;
     case VFR_OPT_BLOCKS_PER_SM: C.tune.blocks_per_sm = (uint32_t)value; return VFR_OK;
     case VFR_OPT_PROFILE: C.profile = value != 0; return VFR_OK;
+    case VFR_OPT_TRAVERSE_VARIANT:
+      if (value > 1) return C.fail(VFR_ERR_INVALID, "traversal variant is 0 or 1");
+      C.tune.variant = (uint32_t)value;
+      return VFR_OK;
+    case VFR_OPT_REFILL:
+      if (value < 1 || value > 32) return C.fail(VFR_ERR_INVALID, "refill is 1..32");
+      C.tune.refill = (uint32_t)value;
+      return VFR_OK;
     default: return C.fail(VFR_ERR_INVALID, "unknown option");
   }
 }
@@ -351,6 +362,7 @@ int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
     if (!rc) rc = C.cuda(cudaMalloc(&C.d_psi, sizeof(float) * 512 * 512), "psi alloc");
     if (rc) return rc;
   }
+  C.psi_one = psi[0] == 1.0f;
   int rc = C.cuda(cudaMemcpyAsync(C.d_tf, tf, sizeof(float) * 1024, cudaMemcpyHostToDevice, C.stream),
                   "tf upload");
   if (!rc)
@@ -370,21 +382,22 @@ int vfr_mesh_upload(vfr_ctx* c, const float* vert4, uint32_t nV, const uint32_t*
   if ((uint64_t)nExt > 4ull * nT) return C.fail(VFR_ERR_INVALID, "more external faces than faces");
   std::string why;
   if (!vfr::validate_mesh(tet4, con4, nV, nT, extf2, nExt, why)) return C.fail(VFR_ERR_MESH, why);
-  std::vector<vfr::TetRec> rec(nT);
-  for (size_t t = 0; t < nT; ++t) {
-    rec[t].v = make_uint4(tet4[4 * t], tet4[4 * t + 1], tet4[4 * t + 2], tet4[4 * t + 3]);
-    rec[t].n = make_uint4(con4[4 * t], con4[4 * t + 1], con4[4 * t + 2], con4[4 * t + 3]);
-  }
+  std::vector<uint32_t> walk(8 * (size_t)nT);
+  if (!vfr::build_walk(tet4, con4, nV, nT, walk.data(), why)) return C.fail(VFR_ERR_MESH, why);
   std::unique_ptr<Mesh> m(new Mesh);
   m->nV = nV; m->nT = nT; m->nExt = nExt;
   m->maxEdge = maxEdge; m->maxZ = maxZ; m->minZ = minZ;
-  int rc = C.cuda(cudaMalloc(&m->rec, sizeof(vfr::TetRec) * (size_t)nT), "tet records");
+  int rc = C.cuda(cudaMalloc(&m->tet, sizeof(uint4) * (size_t)nT), "tets");
+  if (!rc) rc = C.cuda(cudaMalloc(&m->walk, sizeof(vfr::WalkRec) * (size_t)nT), "walk records");
   if (!rc) rc = C.cuda(cudaMalloc(&m->vert, sizeof(float4) * (size_t)nV), "vertices");
   if (!rc) rc = C.cuda(cudaMalloc(&m->extf, sizeof(uint2) * std::max<size_t>(nExt, 1)), "ext faces");
   if (!rc)
-    rc = C.cuda(cudaMemcpy(m->rec, rec.data(), sizeof(vfr::TetRec) * (size_t)nT,
+    rc = C.cuda(cudaMemcpy(m->tet, tet4, sizeof(uint4) * (size_t)nT, cudaMemcpyHostToDevice),
+                "tet upload");
+  if (!rc)
+    rc = C.cuda(cudaMemcpy(m->walk, walk.data(), sizeof(vfr::WalkRec) * (size_t)nT,
                            cudaMemcpyHostToDevice),
-                "record upload");
+                "walk upload");
   if (!rc)
     rc = C.cuda(cudaMemcpy(m->vert, vert4, sizeof(float4) * (size_t)nV, cudaMemcpyHostToDevice),
                 "vertex upload");
@@ -392,7 +405,7 @@ int vfr_mesh_upload(vfr_ctx* c, const float* vert4, uint32_t nV, const uint32_t*
     rc = C.cuda(cudaMemcpy(m->extf, extf2, sizeof(uint2) * (size_t)nExt, cudaMemcpyHostToDevice),
                 "ext-face upload");
   if (rc) return rc;
-  m->bytes = sizeof(vfr::TetRec) * (size_t)nT + sizeof(float4) * (size_t)nV +
+  m->bytes = (sizeof(uint4) + sizeof(vfr::WalkRec)) * (size_t)nT + sizeof(float4) * (size_t)nV +
              sizeof(uint2) * (size_t)nExt;
   for (size_t i = 0; i < C.meshes.size(); ++i)
     if (!C.meshes[i]) {

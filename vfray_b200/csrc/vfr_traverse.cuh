@@ -1,0 +1,311 @@
+// Stage (c): tet-to-tet traversal with partial pre-integration
+// (vfRayKernelCPU.cc:173-566), one lane per ray, persistent warps.
+//
+// Per-lane state machine: a lane walks one tet per loop iteration; when its
+// ray ends it writes the pixel and the warp refills idle lanes from the
+// view's ray queue (one warp-aggregated atomicAdd), so lanes do not wait for
+// the longest ray of their warp.  The current tet's 4 vertices live in
+// registers rotated by the entry face f (r_j = local vertex (f + j) & 3), so
+// the three exit candidates (f+1, f+2, f+3) read fixed registers: candidate
+// i uses (r_i, r_i+1, r_i+2).  Once the exit face is known, a step issues its
+// two loads together: the next tet's 32-byte walk record and the one vertex
+// the next tet does not share with this one (its id is in this tet's record),
+// so one memory round trip per step.
+#pragma once
+#include "vfr_device.cuh"
+
+namespace vfr {
+
+// One exit candidate (vfRayKernelCPU.cc:312-348), branch-free.  The slack
+// test (double)(c1+c2) <= (double)cr + 1e-12 is decided in float unless cr is
+// below 2^-16: for larger cr the next float above cr is more than 1e-12 away.
+__device__ __forceinline__ bool exit_test(const float4& a, const float4& b, const float4& c,
+                                          float ox, float oy) {
+  const float v1x = fsub(b.x, a.x), v1y = fsub(b.y, a.y);
+  const float v2x = fsub(c.x, a.x), v2y = fsub(c.y, a.y);
+  float cr = fsub(fmul(v1x, v2y), fmul(v1y, v2x));
+  const bool skip = below_rdelta(cr);
+  const bool neg = cr < 0.0f;
+  const float w1x = neg ? v2x : v1x, w1y = neg ? v2y : v1y;
+  const float w2x = neg ? v1x : v2x, w2y = neg ? v1y : v2y;
+  cr = neg ? -cr : cr;
+  const float v0x = fsub(ox, a.x), v0y = fsub(oy, a.y);
+  const float c1 = fsub(fmul(w1x, v0y), fmul(w1y, v0x));
+  const float c2 = fsub(fmul(v0x, w2y), fmul(v0y, w2x));
+  const float sum = fadd(c1, c2);
+  const bool within = (sum <= cr) ||
+                      (cr < 1.52587890625e-05f && (double)sum <= dadd((double)cr, kRDelta));
+  return !skip && (c1 >= 0.0f) && (c2 >= 0.0f) && within;
+}
+
+__device__ __forceinline__ float4 pick3(uint32_t i, const float4& x1, const float4& x2,
+                                        const float4& x3) {
+  float4 r = x3;
+  if (i == 1) r = x1;
+  if (i == 2) r = x2;
+  return r;
+}
+__device__ __forceinline__ uint32_t pick3u(uint32_t i, uint32_t x1, uint32_t x2, uint32_t x3) {
+  return i == 1 ? x1 : (i == 2 ? x2 : x3);
+}
+
+struct Ray {
+  float4 r0, r1, r2, r3;       // vertices rotated by the entry face
+  WalkRec w;                   // walk record of the current tet
+  float4 cb;                   // colorBack
+  uint32_t t, f, p, iters;
+  float ox, oy, zp, sp;
+  float ar, ag, ab, tr, lastZ;
+  // composited mode: this pixel's entry list and the last entry taken
+  uint32_t ea, en, dz_bits, de;
+  float exitZ;
+};
+
+// Start a segment at external face e with entry depth zp (:256-279).
+__device__ __forceinline__ void begin_segment(const TraverseParams& P, const float4* s_tf, Ray& R,
+                                              uint32_t e, float zp, float sp) {
+  const uint2 tf = P.extf[e];
+  R.t = tf.x;
+  R.f = tf.y;
+  const uint4 id = P.tet[R.t];
+  R.w = P.walk[R.t];
+  R.r0 = P.vert[sel4(id, R.f)];
+  R.r1 = P.vert[sel4(id, (R.f + 1) & 3u)];
+  R.r2 = P.vert[sel4(id, (R.f + 2) & 3u)];
+  R.r3 = P.vert[sel4(id, (R.f + 3) & 3u)];
+  R.zp = zp;
+  R.sp = sp;
+  R.lastZ = zp;
+  R.cb = s_tf[(uint32_t)fmul(255.0f, sp)];
+}
+
+// Composited mode: the next entry of the pixel in (depth, index) descending
+// order after the last one taken, skipping entries above the depth where the
+// previous segment left the mesh.  Returns false when the list is done.
+__device__ __forceinline__ bool next_entry(const TraverseParams& P, const float4* s_tf, Ray& R,
+                                           bool first) {
+  for (;;) {
+    float bz = -INFINITY;
+    uint32_t be = 0, bzb = 0;
+    bool found = false;
+    const float dzl = __uint_as_float(R.dz_bits);
+    for (uint32_t k = 0; k < R.en; ++k) {
+      const uint2 q = P.ent[R.ea + k];
+      const float z = __uint_as_float(q.x);
+      const bool below = first || (z < dzl) || (z == dzl && q.y < R.de);
+      if (!below) continue;
+      if (!found || z > bz || (z == bz && q.y > be)) {
+        bz = z;
+        be = q.y;
+        bzb = q.x;
+        found = true;
+      }
+    }
+    if (!found) return false;
+    R.dz_bits = bzb;
+    R.de = be;
+    first = false;
+    if (bz > R.exitZ) continue;  // behind the ray already
+    const float4 p0 = P.planes[2 * (size_t)be], p1 = P.planes[2 * (size_t)be + 1];
+    begin_segment(P, s_tf, R, be, bz, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
+    return true;
+  }
+}
+
+__device__ __forceinline__ void finish_pixel(const TraverseParams& P, const Ray& R) {
+  float c[3] = {R.ar, R.ag, R.ab};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) c[k] = (c[k] > 1.0f) ? 1.0f : c[k];  // :546-548
+  if (P.rgb8) {
+    uint8_t* o = P.rgb8 + 3 * (size_t)R.p;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o[k] = (uint8_t)__float2int_rz(fmul(255.0f, c[k]));  // :550-552
+  }
+  if (P.rgba) P.rgba[R.p] = make_float4(c[0], c[1], c[2], fsub(1.0f, R.tr));
+  if (P.steps) P.steps[R.p] = R.iters;
+}
+
+enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kAbandon = 2, kCap = 3, kRange = 4 };
+
+// One iteration of the reference's while loop (:302-542).
+__device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* s_tf, float maxEdge,
+                                         bool psi_one, Ray& R) {
+  if (++R.iters > P.step_cap) return kCap;
+  const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
+  const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
+  const bool h3 = exit_test(R.r3, R.r0, R.r1, R.ox, R.oy);
+  const uint32_t i = h1 ? 1u : (h2 ? 2u : (h3 ? 3u : 0u));
+  if (i == 0) return kSegmentEnd;  // :353 no exit face
+  const uint32_t ex = (R.f + i) & 3u;
+  const uint32_t tn = sel4(R.w.n, ex);
+  const uint32_t q = sel4(R.w.q, ex);
+  const bool leaving = (tn == R.t);
+  if (tn >= P.nT) return kRange;
+  // both loads of the step, issued before the plane solve that hides them
+  WalkRec N = R.w;
+  float4 nv = R.r0;
+  if (!leaving) {
+    N = P.walk[tn];
+    nv = P.vert[q & 0x07ffffffu];
+  }
+  // exit face (ex, ex+1, ex+2) = (r_i, r_i+1, r_i+2)
+  const float4 a = pick3(i, R.r1, R.r2, R.r3);
+  const float4 b = pick3(i, R.r2, R.r3, R.r0);
+  const float4 c = pick3(i, R.r3, R.r0, R.r1);
+  Plane nf;
+  face_plane(a, b, c, nf);
+  const float zn = plane_eval(R.ox, R.oy, nf.zx, nf.zy, nf.zz);
+  const float sn = plane_eval(R.ox, R.oy, nf.sx, nf.sy, nf.sz);
+  float dz = fsub(R.zp, zn);
+  dz = dz < 0.0f ? -dz : dz;
+  dz = below_rdelta(dz) ? 0.0f : dz;
+  if ((sn < 0.0f) || (sn > 1.0f)) return kSegmentEnd;  // :446
+  dz = (dz == 0.0f) ? 0.0f : fdiv(dz, maxEdge);
+  const float4 cf = s_tf[(uint32_t)fmul(255.0f, sn)];
+  const float taux = fmul(cf.w, dz), tauy = fmul(R.cb.w, dz);
+  if (!(psi_one && taux == 0.0f && tauy == 0.0f)) {
+    // With both extinctions 0: zeta = 1, gamma = 0, psi = table[0][0] = 1,
+    // so the colour term is 0 and 1 - alpha = 1: the sum is unchanged, and
+    // the step can skip to the colour hand-over (psi_one: table[0][0] == 1).
+    const float zeta = (float)exp(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)));
+    // tau / (1.0 + tau) in double; a zero numerator is taken apart so that
+    // the division never meets its special-case path
+    const double tx1 = taux == 0.0f ? 1.0 : (double)taux;
+    const double ty1 = tauy == 0.0f ? 1.0 : (double)tauy;
+    const float gx = taux == 0.0f ? 0.0f : (float)ddiv(tx1, dadd(1.0, tx1));
+    const float gy = tauy == 0.0f ? 0.0f : (float)ddiv(ty1, dadd(1.0, ty1));
+    // gamma + 0.5/512: a float plus an exactly representable constant,
+    // rounded once to float either way (double rounding of + is innocuous)
+    const float tcx = fadd(gx, 0.5f / 512.0f), tcy = fadd(gy, 0.5f / 512.0f);
+    if ((tcx < 0.0f) || (tcx > 1.0f) || (tcy < 0.0f) || (tcy > 1.0f)) return kSegmentEnd;  // :468
+    const uint32_t pi = min((uint32_t)fmul(tcx, 512.0f), 511u);
+    const uint32_t pj = min((uint32_t)fmul(tcy, 512.0f), 511u);
+    const double psi = (double)__ldg(P.psi + pi * 512u + pj);
+    const double dzeta = (double)zeta;
+    const double ca = dsub(1.0, psi), cbk = dsub(psi, dzeta);
+    const float fr = (float)dadd(dmul((double)cf.x, ca), dmul((double)R.cb.x, cbk));
+    const float fg = (float)dadd(dmul((double)cf.y, ca), dmul((double)R.cb.y, cbk));
+    const float fb = (float)dadd(dmul((double)cf.z, ca), dmul((double)R.cb.z, cbk));
+    const float fw = fsub(1.0f, zeta);           // (float)(1.0 - zeta), innocuous double rounding
+    const double keep = dsub(1.0, (double)fw);   // exact
+    R.ar = (float)dadd((double)fr, dmul(keep, (double)R.ar));
+    R.ag = (float)dadd((double)fg, dmul(keep, (double)R.ag));
+    R.ab = (float)dadd((double)fb, dmul(keep, (double)R.ab));
+    R.tr = fmul(R.tr, zeta);
+  }
+  R.lastZ = zn;
+  R.cb = cf;
+  if (leaving) return kSegmentEnd;  // :535
+  // advance to tn through its face fn: slots fn..fn+2 are the exit face's
+  // vertices in tn's order (permutation code), slot fn+3 is the loaded vertex
+  const uint32_t fn = (q >> 27) & 3u, code = q >> 29;
+  if (code < 6) {
+    const uint32_t pc = perm_code(code);
+    const uint32_t m0 = pc & 3u, m1 = (pc >> 2) & 3u, m2 = (pc >> 4) & 3u;
+    R.r0 = m0 == 0 ? a : (m0 == 1 ? b : c);
+    R.r1 = m1 == 0 ? a : (m1 == 1 ? b : c);
+    R.r2 = m2 == 0 ? a : (m2 == 1 ? b : c);
+    R.r3 = nv;
+  } else {  // shared face not matched by vertex ids: reload the tet's vertices
+    const uint4 id = P.tet[tn];
+    R.r0 = P.vert[sel4(id, fn)];
+    R.r1 = P.vert[sel4(id, (fn + 1) & 3u)];
+    R.r2 = P.vert[sel4(id, (fn + 2) & 3u)];
+    R.r3 = P.vert[sel4(id, (fn + 3) & 3u)];
+  }
+  R.w = N;
+  R.t = tn;
+  R.f = fn;
+  R.zp = zn;
+  R.sp = sn;
+  return kContinue;
+}
+
+// kMinBlocks: CTAs of 256 threads the register budget must allow per SM
+// (2: ~104 registers, no spills; 3: 80 registers, a few spilled to L1).
+template <int kMode, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParams P) {
+  __shared__ float4 s_tf[256];
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tf[i] = P.tf[i];
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const uint32_t nrays = P.ctr->nrays;
+  const float maxEdge = P.use_view_maxedge ? __uint_as_float(P.ctr->maxedge_bits) : P.maxEdge;
+  const uint32_t refill = P.refill ? P.refill : 1u;
+  const bool psi_one = P.psi_one != 0;
+  unsigned long long my_steps = 0;
+  uint32_t status = 0;
+  bool active = false, exhausted = false;
+  Ray R;
+  for (;;) {
+    const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+    if (idle && !exhausted && ((uint32_t)__popc(idle) >= refill || idle == 0xffffffffu)) {
+      const uint32_t leader = __ffs(idle) - 1u, k = __popc(idle);
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(&P.ctr->queue, k);
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (base + k >= nrays) exhausted = true;
+      if (!active) {
+        const uint32_t rr = base + __popc(idle & lt_mask);
+        if (rr < nrays) {
+          R.p = P.rays[rr];
+          const uint32_t x = R.p % P.W, y = R.p / P.W;
+          R.ox = obj_coord(x, P.W);
+          R.oy = obj_coord(y, P.H);
+          R.ar = R.ag = R.ab = 0.0f;
+          R.tr = 1.0f;
+          R.iters = 0;
+          if (kMode == 0) {
+            const uint32_t e = (uint32_t)P.winner[R.p];
+            const float4 p0 = P.planes[2 * (size_t)e], p1 = P.planes[2 * (size_t)e + 1];
+            begin_segment(P, s_tf, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
+                          plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
+            active = true;
+          } else {
+            R.ea = P.ent_off[R.p];
+            const uint32_t b1 = P.ent_off[R.p + 1];
+            R.en = b1 - R.ea;
+            R.exitZ = INFINITY;
+            R.dz_bits = 0;
+            R.de = 0;
+            if (b1 > P.ent_cap) {
+              status |= 16u;  // VFR_DEV_OVERFLOW: the caller renders again with room
+            } else {
+              active = next_entry(P, s_tf, R, true);
+              if (!active) finish_pixel(P, R);
+            }
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (!active) continue;
+    const uint32_t res = step(P, s_tf, maxEdge, psi_one, R);
+    if (res == kContinue) continue;
+    if (res == kSegmentEnd) {
+      if (kMode == 1) {
+        R.exitZ = R.lastZ;
+        if (next_entry(P, s_tf, R, false)) continue;
+      }
+      finish_pixel(P, R);
+    } else if (res == kAbandon) {
+      status |= 1u;  // the reference writes nothing for this pixel (:365)
+    } else if (res == kCap) {
+      status |= 2u;
+      finish_pixel(P, R);
+    } else {
+      status |= 4u;
+    }
+    my_steps += R.iters;
+    active = false;
+  }
+  for (int o = 16; o; o >>= 1) my_steps += __shfl_xor_sync(0xffffffffu, my_steps, o);
+  if (lane == 0 && my_steps) atomicAdd(&P.ctr->steps, my_steps);
+  if (status) atomicOr(&P.ctr->status, status);
+}
+
+}  // namespace vfr
