@@ -155,6 +155,29 @@ VFR_API int vfr_render_device(vfr_ctx* ctx, int mesh_id, const float* mv16, uint
                       int32_t* writer_dev);
 VFR_API int vfr_device_status(vfr_ctx* ctx, uint32_t* status);
 
+/* ---- stage (a) for callers that cannot allocate ------------------------ */
+
+/* No counterpart in the reference.  Stage (a) (findVisibleFaces + ordered
+ * compaction) for callers that must not see the library allocate device
+ * memory: an application that has reserved the GPU's memory for its own pool
+ * (a game engine, a serving process with a fixed budget), or a frame loop in
+ * which cudaMalloc/cudaFree, which may synchronise the device, must not run.
+ * Inputs and outputs are the caller's device buffers (vert4_dev 16-byte
+ * aligned nV x float4, tet4_dev 16-byte aligned nT x uint4, extf2_dev nExt x
+ * uint2); writes visExt_dev (visible ext-face indices in order, capacity
+ * nExt) and *num_vis_dev, asynchronously on `stream` (a cudaStream_t, NULL =
+ * the default stream).  Its scratch is a fixed device array inside the
+ * library (32 bytes per external face for up to VFR_STATIC_MAX_EXT faces,
+ * about 8 MiB, held on every GPU that loads the library until exit); larger
+ * meshes get VFR_ERR_BUDGET.  The first call on a device looks that array's
+ * address up, so make it before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race.  An external face whose ids are out of
+ * range counts as not visible.  Calls no cudaMalloc/cudaFree. */
+#define VFR_STATIC_MAX_EXT (1u << 18)
+VFR_API int vfr_find_visible_static(const float* vert4_dev, uint32_t nV, const uint32_t* tet4_dev,
+                                    uint32_t nT, const uint32_t* extf2_dev, uint32_t nExt,
+                                    uint32_t* visExt_dev, uint32_t* num_vis_dev, void* stream);
+
 /* ---- host-side precomputation and files (vfRayPreComp.h:97-279) -------- */
 
 /* The psi(gamma) table this library generates: psi(tf, tb) =

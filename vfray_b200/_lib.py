@@ -84,6 +84,7 @@ SIGNATURES = {
     "vfr_render": (_i, [_vp, _i, _vp, _u32, _u32, _i, _vp, _vp, _vp, C.POINTER(RenderStats)]),
     "vfr_render_device": (_i, [_vp, _i, _vp, _u32, _u32, _i, _vp, _vp, _vp, _vp]),
     "vfr_device_status": (_i, [_vp, C.POINTER(_u32)]),
+    "vfr_find_visible_static": (_i, [_vp, _u32, _vp, _u32, _vp, _u32, _vp, _vp, _vp]),
     "vfr_psi_table": (_i, [_vp]),
     "vfr_normalize": (_i, [_vp, _u32]),
     "vfr_rotate": (_i, [_vp, _u32, _vp]),
