@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain", choices=["batched", "plain"])
+    ap.add_argument("--form", default="batched", choices=["batched", "plain"])
     ap.add_argument("--workload", default="orbit64", choices=["orbit64", "convex24"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="bound of the CPU-baseline sample")
@@ -191,7 +191,7 @@ def run_ours(args, rank, world, dist):
         def step_plain_or_batched():
             for i, mv in enumerate(views):
                 r.render_device(mid, W, H, mv=mv, rgb8=rgb_d[i], rgba=rgba_d[i])
-        launches_per_step = 9 * nv
+        launches_per_step = 11 * nv
 
     def plain_step():
         for i, mv in enumerate(views):
@@ -226,7 +226,21 @@ def run_ours(args, rank, world, dist):
         dist.barrier()
     with Clocks(dev) as clk:
         t_main, _ = timed(step_plain_or_batched, args.steps, args.warmup)
-    t_plain, prof = timed(plain_step, max(1, min(args.steps, 3)), 1, profile=True)
+    if args.form == "batched":
+        bst = runner.stats()  # raises on any device status of the batch
+        assert sum(x["num_rays"] for x in bst) == rays_step, "batched rays differ from single views"
+        assert sum(x["num_steps"] for x in bst) == steps_step, "batched steps differ"
+    t_plain, prof_plain = timed(plain_step, max(1, min(args.steps, 3)), 1, profile=True)
+    if args.form == "batched":
+        # stage times of the batched chain: the same batch launched directly
+        # (not as a graph) with events between its stages
+        runner_p = vbatch.BatchRenderer(r, [(mid, mv, W, H) for mv in views], graph=False)
+        _, prof = timed(lambda: runner_p.run(), max(1, min(args.steps, 3)), 1, profile=True)
+        runner_p.close()
+        launches_per_trav = 1
+    else:
+        prof = prof_plain
+        launches_per_trav = nv
 
     # e2e through the host API: camera in, RGB8 out (pinned), copies timed
     pinned = torch.empty((nv, H, W, 3), dtype=torch.uint8, pin_memory=True)
@@ -259,23 +273,30 @@ def run_ours(args, rank, world, dist):
     e2e = rays_step * world * K / (t_e2e * 1e-3) / 1e6
     plain = rays_step * world * max(1, min(K, 3)) / (t_plain * 1e-3) / 1e6
 
-    # roofline of the traversal kernel (per launch = per view)
+    # roofline of the traversal kernel: algorithmic bytes of a launch over its
+    # event-timed duration (batched: one launch covers all views)
     peak, peak_kind = load_peaks()
     trav_ms = prof[:, 2] if prof is not None and len(prof) else None
     roof = None
     if trav_ms is not None:
-        nrep = len(trav_ms) // nv
-        bytes_total = BYTES_PER_STEP * steps_step * nrep
-        achieved = bytes_total / (trav_ms.sum() * 1e-3) / 1e9
+        bytes_per_launch = BYTES_PER_STEP * steps_step / launches_per_trav
+        achieved = bytes_per_launch * len(trav_ms) / (trav_ms.sum() * 1e-3) / 1e9
         traffic = load_traffic()
-        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
-                if peak_kind == "measured" else "fallback 6.65 TB/s",
+        roof = {"bound": "hbm", "achieved": round(float(achieved), 1), "peak": peak, "unit": "GB/s",
+                "frac": round(float(achieved / peak), 4),
+                "peak_kind": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                              else "fallback 6.65 TB/s"),
                 "traffic": None if traffic is None else traffic.get("bytes_per_launch"),
-                "algorithmic_bytes_per_launch": int(BYTES_PER_STEP * steps_step / nv),
-                "kernel": "traverse_kernel<0>",
+                "algorithmic_bytes_per_launch": int(bytes_per_launch),
+                "bytes_per_step": BYTES_PER_STEP,
+                "kernel": "vfr::traverse_kernel<0,2>" + (" (one launch for all views)"
+                                                        if launches_per_trav == 1 else " (per view)"),
                 "launch_ms_mean": round(float(trav_ms.mean()), 4),
+                "gsteps_per_s": round(float(steps_step / launches_per_trav * len(trav_ms)
+                                            / (trav_ms.sum() * 1e-3) / 1e9), 2),
                 "stage_ms_mean": [round(float(x), 4) for x in prof.mean(0)]}
+    if args.form == "batched":
+        runner.close()
     r.release_mesh(mid)
     r.close()
     if rank != 0:
@@ -400,6 +421,9 @@ def _json(o):
 
 
 def main():
+    import faulthandler
+
+    faulthandler.enable()
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

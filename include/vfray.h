@@ -54,7 +54,8 @@ extern "C" {
 #define VFR_OPT_BLOCKS_PER_SM 3   /* traversal CTAs per SM; 0 = occupancy maximum */
 #define VFR_OPT_PROFILE 4         /* 1: record per-stage CUDA events of every view */
 #define VFR_OPT_TRAVERSE_VARIANT 5 /* traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM */
-#define VFR_OPT_REFILL 6          /* refill a warp's idle lanes once >= this many are idle (1) */
+#define VFR_OPT_REFILL 6          /* refill a warp's idle lanes once >= this many are idle (4) */
+#define VFR_OPT_RASTER_WARPS 7    /* stage (b) warps per SM (64) */
 
 /* Render modes. */
 #define VFR_MODE_REF 0        /* reference semantics: last visible face wins each pixel */
@@ -154,6 +155,45 @@ VFR_API int vfr_render_device(vfr_ctx* ctx, int mesh_id, const float* mv16, uint
                       int mode, uint8_t* rgb8_dev, float* rgba_dev, uint32_t* steps_dev,
                       int32_t* writer_dev);
 VFR_API int vfr_device_status(vfr_ctx* ctx, uint32_t* status);
+
+/* ---- batches: many (mesh, camera, resolution) views in one launch chain -- */
+
+/* No single counterpart in the reference, whose driver renders one view per
+ * call (vfRay.cu:618-641 re-runs the three kernels for each rotation).  A
+ * batch lays out all jobs in shared device arenas; each stage is one launch
+ * over all jobs, and the traversal is one persistent launch whose warps take
+ * rays of any job from one device work queue.  The chain can be captured
+ * once as a CUDA graph and replayed. */
+typedef struct {
+  int mesh_id;
+  uint32_t W, H;
+  int use_mv;          /* 1: rotate + normalise + recompute the limits with mv */
+  float mv[16];        /* row-major model-view (rotateVolume's layout) */
+  uint8_t* rgb8_dev;   /* device outputs; all three NULL: the batch owns them */
+  float* rgba_dev;
+  uint32_t* steps_dev;
+} vfr_job;
+
+typedef struct vfr_batch vfr_batch;
+VFR_API int vfr_batch_create(vfr_ctx* ctx, vfr_batch** out);
+VFR_API void vfr_batch_destroy(vfr_batch* b);
+/* Lays out (allocating) and uploads the jobs; mode is for all jobs. */
+VFR_API int vfr_batch_set_jobs(vfr_batch* b, const vfr_job* jobs, uint32_t n, int mode);
+/* Captures the whole chain as a CUDA graph; vfr_batch_run then replays it. */
+VFR_API int vfr_batch_capture(vfr_batch* b);
+/* Enqueues the batch on the context stream (asynchronous). */
+VFR_API int vfr_batch_run(vfr_batch* b);
+/* Waits, then fills per-job stats (n entries at most); returns the status. */
+VFR_API int vfr_batch_stats(vfr_batch* b, vfr_render_stats* per_job, uint32_t n);
+/* Device output pointers of a job (the batch's own when it owns them). */
+VFR_API int vfr_batch_output(vfr_batch* b, uint32_t job, uint8_t** rgb8_dev, float** rgba_dev,
+                             uint32_t** steps_dev);
+/* Copies every job's outputs to host buffers, concatenated in job order
+ * (any may be NULL), and waits: the host-buffer end of a batch. */
+VFR_API int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host,
+                           uint32_t* steps_host);
+/* Device bytes of the batch's scratch arenas. */
+VFR_API int vfr_batch_scratch_bytes(vfr_batch* b, uint64_t* bytes);
 
 /* ---- stage (a) for callers that cannot allocate ------------------------ */
 

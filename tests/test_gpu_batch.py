@@ -1,0 +1,91 @@
+"""Batched form: every job of a batch (mixed meshes, resolutions, cameras,
+run directly or as a captured CUDA graph) gives exactly the image and tet-walk
+lengths of the same view rendered alone, which the parity tests tie to the
+reference."""
+import numpy as np
+import pytest
+
+import vfray_b200 as vb
+from vfray_b200 import batch as vbatch
+from vfray_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def scene(renderer):
+    meshes = []
+    for n, carved, seed in [(10, True, 4), (7, False, 5)]:
+        vert, tet = synth.make_mesh(n, carved=carved, view_seed=None)
+        p = vb.prepare(vert, tet)
+        renderer.upload_tables(synth.transfer_function(2))
+        meshes.append(renderer.upload_mesh(p["vert"], p["tet"], p["con"], p["extf"], p["lmt"]))
+    views = synth.orbit_views(5, seed=9)
+    jobs = [(meshes[0], views[0], 96, 80), (meshes[1], views[1], 64, 64),
+            (meshes[0], None, 50, 37), (meshes[0], views[2], 128, 128),
+            (meshes[1], views[3], 33, 90), (meshes[1], None, 64, 64)]
+    yield jobs
+    for m in meshes:
+        renderer.release_mesh(m)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("mode", [vb.MODE_REF, vb.MODE_COMPOSITED])
+def test_batch_equals_single_views(renderer, scene, graph, mode):
+    B = vbatch.BatchRenderer(renderer, scene, mode=mode, graph=graph)
+    try:
+        B.prepare()
+        for rep in range(2):  # a replayed graph gives the same result
+            B.run()
+            stats = B.stats()
+            npx = sum(W * H for (_, _, W, H) in scene)
+            rgb = np.empty(npx * 3, np.uint8)
+            steps = np.empty(npx, np.uint32)
+            B.read(rgb8=rgb, steps=steps)
+            off = 0
+            for j, (mid, mv, W, H) in enumerate(scene):
+                single = renderer.render(mid, W, H, mv=mv, mode=mode)
+                n = W * H
+                assert np.array_equal(rgb[3 * off:3 * (off + n)].reshape(H, W, 3), single["rgb8"]), j
+                assert np.array_equal(steps[off:off + n].reshape(H, W), single["steps"]), j
+                assert stats[j]["num_rays"] == single["stats"]["num_rays"]
+                assert stats[j]["num_steps"] == single["stats"]["num_steps"]
+                off += n
+    finally:
+        B.close()
+
+
+def test_batch_device_outputs(renderer, scene):
+    """Jobs may render into the caller's device buffers."""
+    import torch
+
+    jobs, bufs = [], []
+    for (mid, mv, W, H) in scene:
+        rgb = torch.full((H, W, 3), 7, dtype=torch.uint8, device="cuda")
+        bufs.append(rgb)
+        jobs.append(vbatch.job(mid, W, H, mv=mv, rgb8=rgb))
+    B = vbatch.BatchRenderer(renderer, jobs)
+    try:
+        B.prepare()
+        B.run()
+        B.stats()
+        for (mid, mv, W, H), rgb in zip(scene, bufs):
+            single = renderer.render(mid, W, H, mv=mv)
+            assert np.array_equal(rgb.cpu().numpy(), single["rgb8"])
+    finally:
+        B.close()
+
+
+def test_batch_outliving_its_context_is_safe():
+    """Destroying the context first detaches its batches: running one then
+    reports a state error, and destroying it is still safe."""
+    p = vb.prepare(*synth.make_mesh(4, view_seed=1))
+    r = vb.Renderer(0)
+    r.upload_tables(synth.transfer_function(2))
+    mid = r.upload_mesh(p["vert"], p["tet"], p["con"], p["extf"], p["lmt"])
+    B = vbatch.BatchRenderer(r, [(mid, None, 16, 16)], graph=False)
+    B.run()
+    B.stats()
+    r.close()
+    assert B.lib.vfr_batch_run(B.h) == vb._lib.VFR_ERR_STATE
+    B.close()

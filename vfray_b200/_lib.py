@@ -37,6 +37,7 @@ OPT_BLOCKS_PER_SM = 3
 OPT_PROFILE = 4
 OPT_TRAVERSE_VARIANT = 5
 OPT_REFILL = 6
+OPT_RASTER_WARPS = 7
 
 MODE_REF = 0
 MODE_COMPOSITED = 1
@@ -56,6 +57,13 @@ class RenderStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Job(C.Structure):
+    """vfr_job of include/vfray.h."""
+    _fields_ = [("mesh_id", C.c_int), ("W", C.c_uint32), ("H", C.c_uint32), ("use_mv", C.c_int),
+                ("mv", C.c_float * 16), ("rgb8_dev", C.c_void_p), ("rgba_dev", C.c_void_p),
+                ("steps_dev", C.c_void_p)]
 
 
 _vp = C.c_void_p
@@ -84,6 +92,15 @@ SIGNATURES = {
     "vfr_render": (_i, [_vp, _i, _vp, _u32, _u32, _i, _vp, _vp, _vp, C.POINTER(RenderStats)]),
     "vfr_render_device": (_i, [_vp, _i, _vp, _u32, _u32, _i, _vp, _vp, _vp, _vp]),
     "vfr_device_status": (_i, [_vp, C.POINTER(_u32)]),
+    "vfr_batch_create": (_i, [_vp, C.POINTER(_vp)]),
+    "vfr_batch_destroy": (None, [_vp]),
+    "vfr_batch_set_jobs": (_i, [_vp, C.POINTER(Job), _u32, _i]),
+    "vfr_batch_capture": (_i, [_vp]),
+    "vfr_batch_run": (_i, [_vp]),
+    "vfr_batch_stats": (_i, [_vp, C.POINTER(RenderStats), _u32]),
+    "vfr_batch_output": (_i, [_vp, _u32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
+    "vfr_batch_read": (_i, [_vp, _vp, _vp, _vp]),
+    "vfr_batch_scratch_bytes": (_i, [_vp, C.POINTER(C.c_uint64)]),
     "vfr_find_visible_static": (_i, [_vp, _u32, _vp, _u32, _vp, _u32, _vp, _vp, _vp]),
     "vfr_psi_table": (_i, [_vp]),
     "vfr_normalize": (_i, [_vp, _u32]),

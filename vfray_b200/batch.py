@@ -1,0 +1,111 @@
+"""Batched form: many (mesh, camera, resolution) views rendered by one chain
+of launches (vfr_batch_* in include/vfray.h), optionally captured as a CUDA
+graph, with the traversal as one persistent launch pulling rays of every
+view from one device work queue."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import Job, RenderStats, check, ptr
+
+__all__ = ["BatchRenderer", "job"]
+
+
+def job(mesh_id: int, W: int, H: int, mv=None, rgb8=None, rgba=None, steps=None) -> Job:
+    """A vfr_job; outputs are device buffers (torch CUDA tensors) or None
+    (then the batch owns its outputs when all three are None)."""
+    j = Job()
+    j.mesh_id = mesh_id
+    j.W = W
+    j.H = H
+    j.use_mv = 0 if mv is None else 1
+    if mv is not None:
+        m = np.ascontiguousarray(mv, np.float32).reshape(16)
+        for k in range(16):
+            j.mv[k] = float(m[k])
+    j.rgb8_dev = None if rgb8 is None else rgb8.data_ptr()
+    j.rgba_dev = None if rgba is None else rgba.data_ptr()
+    j.steps_dev = None if steps is None else steps.data_ptr()
+    return j
+
+
+class BatchRenderer:
+    """A batch on a Renderer's context.  ``jobs`` are vfr_job structures (see
+    ``job``) or tuples (mesh_id, mv, W, H) rendered into outputs the batch
+    owns."""
+
+    def __init__(self, renderer, jobs, mode: int = _lib.MODE_REF, graph: bool = True):
+        self.r = renderer
+        self.lib = renderer.lib
+        h = C.c_void_p()
+        check(self.lib.vfr_batch_create(renderer.h, C.byref(h)), renderer.h, "vfr_batch_create")
+        self.h = h
+        self.mode = mode
+        self.graph = graph
+        self.set_jobs(jobs)
+
+    def set_jobs(self, jobs):
+        js = [j if isinstance(j, Job) else job(j[0], j[2], j[3], mv=j[1]) for j in jobs]
+        self.jobs = js
+        arr = (Job * len(js))(*js)
+        self._arr = arr
+        check(self.lib.vfr_batch_set_jobs(self.h, arr, len(js), self.mode), self.r.h,
+              "vfr_batch_set_jobs")
+        self.captured = False
+
+    def prepare(self):
+        """Capture the chain as a CUDA graph (once)."""
+        if self.graph and not self.captured:
+            check(self.lib.vfr_batch_capture(self.h), self.r.h, "vfr_batch_capture")
+            self.captured = True
+
+    def run(self, *unused):
+        """Enqueue the batch (asynchronous on the renderer's stream)."""
+        check(self.lib.vfr_batch_run(self.h), self.r.h, "vfr_batch_run")
+
+    def stats(self):
+        """Wait; per-job stats as dicts.  Raises on a device status."""
+        n = len(self.jobs)
+        st = (RenderStats * n)()
+        check(self.lib.vfr_batch_stats(self.h, st, n), self.r.h, "vfr_batch_stats")
+        return [s.as_dict() for s in st]
+
+    def output_ptrs(self, j: int):
+        a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(self.lib.vfr_batch_output(self.h, j, C.byref(a), C.byref(b), C.byref(c)), self.r.h,
+              "vfr_batch_output")
+        return a.value, b.value, c.value
+
+    def scratch_bytes(self) -> int:
+        b = C.c_uint64()
+        check(self.lib.vfr_batch_scratch_bytes(self.h, C.byref(b)), self.r.h,
+              "vfr_batch_scratch_bytes")
+        return int(b.value)
+
+    def launches_per_run(self) -> int:
+        # init, rotate, normalize, maxedge, visible, compact, prefix, raster,
+        # raylist, prefix, traverse (composited: + 2 raster passes, 2 scans, totals)
+        return 11 if self.mode == _lib.MODE_REF else 16
+
+    def read(self, rgb8=None, rgba=None, steps=None):
+        """Copy every job's outputs (concatenated in job order) into host
+        buffers (numpy arrays or pinned torch tensors) and wait."""
+        check(self.lib.vfr_batch_read(self.h, ptr(rgb8), ptr(rgba), ptr(steps)), self.r.h,
+              "vfr_batch_read")
+
+    def run_host(self, rgb8_host):
+        """The host-buffer form: run, then read every job's RGB8 (pinned host
+        memory gives full copy bandwidth)."""
+        self.run()
+        self.read(rgb8=rgb8_host)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.vfr_batch_destroy(self.h)  # safe after the renderer closed too
+            self.h = None
+
+    def __del__(self):
+        self.close()

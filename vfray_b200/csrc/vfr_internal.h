@@ -8,7 +8,7 @@
 #include <vector>
 
 #include "vfr_host.h"
-#include "vfr_kernels.cuh"
+#include "vfr_traverse.cuh"
 
 namespace vfr {
 
@@ -22,9 +22,13 @@ struct Buf {
   ~Buf() {
     if (p) cudaFree(p);
   }
+  template <class T>
+  T* as(size_t byte_off = 0) const {
+    return reinterpret_cast<T*>(static_cast<char*>(p) + byte_off);
+  }
 };
 
-// A resident mesh: packed 32-byte tet records, float4 vertices, ext faces.
+// A resident mesh: tets, walk records, vertices, external faces.
 struct Mesh {
   uint32_t nV = 0, nT = 0, nExt = 0;
   float maxEdge = 0, maxZ = 0, minZ = 0;
@@ -41,33 +45,68 @@ struct Mesh {
   }
 };
 
-// Scratch and state of one view in flight.
-struct View {
-  Mesh* mesh = nullptr;
-  const float4* vert = nullptr;
-  float maxEdge = 0;
-  int use_view_maxedge = 0;
-  uint32_t W = 0, H = 0;
-  int mode = 0;
-  int stage = 0;  // 0 none, 1 visible done, 2 project done
-  ViewCounters* ctr = nullptr;
-  size_t ent_cap = 0;
-  Buf vview, planes, blk, vis_ext, bbox, winner, rays, ent_cnt, ent_off, ent_cur, ent, scan;
-  ~View() {
-    if (ctr) cudaFree(ctr);
-  }
-};
-
 struct Tuning {
-  uint32_t chunk = 32;        // rays per warp fetch from the ray queue
-  uint32_t blocks_per_sm = 0; // traversal CTAs per SM (0: occupancy maximum)
-  uint32_t refill = 1;        // refill idle lanes once this many of a warp's are idle
-  uint32_t variant = 0;       // traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM
+  uint32_t blocks_per_sm = 0;  // traversal CTAs per SM (0: occupancy maximum)
+  uint32_t refill = 4;         // refill idle lanes once this many of a warp's are idle
+  uint32_t variant = 0;        // traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM
+  uint32_t raster_warps_per_sm = 64;
 };
 
-// Four events bracketing the stages of one view (profiling).
-struct StageEvents {
-  cudaEvent_t e[4] = {};
+struct Ctx;
+
+// One render job as the caller describes it.
+struct JobSpec {
+  int mesh = -1;
+  uint32_t W = 0, H = 0;
+  bool use_mv = false;
+  float mv[16] = {};
+  uint8_t* rgb8 = nullptr;  // device outputs (any may be null)
+  float4* rgba = nullptr;
+  uint32_t* steps = nullptr;
+};
+
+// A set of jobs laid out in shared device arenas, run as one chain of
+// launches (optionally a CUDA graph).
+struct Batch {
+  Ctx* ctx = nullptr;
+  int mode = 0;
+  std::vector<JobSpec> specs;
+  std::vector<JobDev> jobs;
+  uint32_t njobs = 0;
+  // host-known prefixes: view blocks, edge blocks, ext-face blocks, tiles
+  std::vector<uint32_t> pref;  // 4 arrays of njobs + 1
+  uint32_t rot_blocks = 0, edge_blocks = 0, ext_blocks = 0, tiles = 0;
+  size_t pixels = 0, ext_total = 0;
+  uint64_t scratch_bytes = 0;
+  Buf d_jobs, d_pref, d_dev_pref, d_ctr;  // d_dev_pref: vis prefix, ray prefix, queue
+  Buf vview, planes, blk, vis, bbox, winner, rays, ent_cnt, ent_off, ent_cur, ent, scan;
+  Buf out_rgb8, out_rgba, out_steps;      // outputs owned by the batch (host-output calls)
+  size_t ent_cap = 0;
+  cudaGraphExec_t exec = nullptr;
+  // pinned staging for the per-call upload of a one-job batch
+  void* stage = nullptr;
+  size_t stage_cap = 0;
+  cudaEvent_t stage_done = nullptr;
+
+  ~Batch();
+  uint32_t* vis_pref() const { return d_dev_pref.as<uint32_t>(); }
+  uint32_t* ray_pref() const { return d_dev_pref.as<uint32_t>((njobs + 1) * 4); }
+  uint32_t* queue() const { return d_dev_pref.as<uint32_t>(2 * (njobs + 1) * 4); }
+  int layout(const std::vector<JobSpec>& s, int mode, bool own_outputs);
+  int upload(bool async);
+  int enqueue_a();
+  int enqueue_b();
+  int enqueue_c();
+  int enqueue_all() {
+    int rc = enqueue_a();
+    if (!rc) rc = enqueue_b();
+    if (!rc) rc = enqueue_c();
+    return rc;
+  }
+  int capture();
+  int run();
+  int counters(std::vector<ViewCounters>& out);
+  void drop_graph();
 };
 
 struct Ctx {
@@ -79,45 +118,29 @@ struct Ctx {
   float* d_psi = nullptr;
   bool psi_one = false;  // psi[0][0] == 1.0f
   std::vector<std::unique_ptr<Mesh>> meshes;
-  View view;
-  Buf out_rgb8, out_rgba, out_steps;
-  ViewCounters* h_ctr = nullptr;
+  Batch plain;     // the one-job batch behind the single-view calls
+  int stage = 0;   // single-view stage calls: 0 none, 1 visible done, 2 project done
   cudaEvent_t ev[4] = {};
   int occ[4] = {0, 0, 0, 0};
   uint32_t step_cap = 0;
   size_t ent_cap_hint = 0;
   Tuning tune;
   bool profile = false;
-  std::vector<StageEvents> prof_pool;  // recycled events
-  std::vector<StageEvents> prof_live;  // recorded, not yet read
-  StageEvents* prof_cur = nullptr;
+  struct StageEvents {
+    cudaEvent_t e[4] = {};
+  };
+  std::vector<StageEvents> prof_pool, prof_live;
+  std::vector<void*> batches;  // live vfr_batch handles, detached when the context goes
+
+  ~Ctx();
   void prof_mark(int k);
-
-  ~Ctx() {
-    meshes.clear();
-    if (d_tf) cudaFree(d_tf);
-    if (d_psi) cudaFree(d_psi);
-    if (h_ctr) cudaFreeHost(h_ctr);
-    for (auto& e : ev)
-      if (e) cudaEventDestroy(e);
-    for (auto* v : {&prof_pool, &prof_live})
-      for (auto& s : *v)
-        for (auto& e : s.e)
-          if (e) cudaEventDestroy(e);
-    if (own_stream) cudaStreamDestroy(own_stream);
-  }
-
   int fail(int code, const std::string& msg);
   int cuda(cudaError_t e, const char* what);
   int grow(Buf& b, size_t bytes, const char* what);
   Mesh* mesh(int id);
-  int enqueue_visible(Mesh& m, const float* mv16, View& v);
-  int enqueue_project(View& v, uint32_t W, uint32_t H, int mode);
-  int enqueue_traverse(View& v, uint8_t* rgb8, float4* rgba, uint32_t* steps);
   int traverse_blocks_per_sm(int mode);
   const void* traverse_fn(int mode, uint32_t variant);
-  int read_counters(View& v, ViewCounters& out);
-  int check_status(const ViewCounters& c);
+  int check_status(uint32_t status, uint32_t nentries_over);
 };
 
 }  // namespace vfr

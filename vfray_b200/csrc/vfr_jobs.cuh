@@ -1,0 +1,480 @@
+// Stages (a) and (b) over a table of render jobs.
+//
+// A job is one (mesh, camera, resolution) view.  Every kernel here covers
+// all jobs of a batch in one launch: items of all jobs share one index space
+// (vertices, tets, external-face blocks, visible faces, screen tiles), and a
+// binary search over a prefix of per-job counts maps an item to its job.
+// Counts known on the host (vertices, tets, faces, tiles) are prefixed on the
+// host; counts produced on the device (visible faces, rays) by
+// prefix_kernel.  Nothing waits on the host between stages, so a batch is one
+// stream-ordered chain of launches (and can be captured as a CUDA graph).
+#pragma once
+#include "vfr_device.cuh"
+
+namespace vfr {
+
+// Per-view device counters.
+struct __align__(16) ViewCounters {
+  uint32_t nvis;             // visible faces
+  uint32_t nrays;            // rays of this job
+  uint32_t nentries;         // entry-list entries (composited mode)
+  uint32_t status;           // VFR_DEV_* bits
+  unsigned long long steps;  // tet-walk iterations of this job's rays
+  uint32_t maxedge_bits;     // view maxEdgeLength (float bits, >= 0)
+  uint32_t pad;
+  uint32_t mm[8];            // orderable min x y z s, max x y z s (view set-up)
+};
+
+// One job as the kernels see it (device memory, uploaded with the batch).
+struct __align__(16) JobDev {
+  float4 m0, m1, m2;         // rows of the model-view (use_mv)
+  const uint4* tet;          // mesh
+  const WalkRec* walk;
+  const float4* vert_in;     // the mesh's (normalised) vertices
+  const uint2* extf;
+  const float4* vert;        // vertices this view renders with (vert_in or vview)
+  float4* vview;             // rotated + normalised vertices (use_mv)
+  float4* planes;            // 2 per external face
+  uint32_t* blk;             // visible count per block of 1024 external faces
+  uint32_t* vis_ext;         // visible external faces, in order
+  uint4* bbox;               // per visible face
+  int32_t* winner;           // W*H, reference mode
+  uint32_t* rays;            // W*H capacity
+  uint32_t* ent_cnt;         // composited: W*H counts (batch arena)
+  uint32_t* ent_off;         // composited: offsets (batch arena, global)
+  uint32_t* ent_cur;
+  ViewCounters* ctr;
+  uint8_t* rgb8;             // outputs (any may be null)
+  float4* rgba;
+  uint32_t* steps;
+  uint32_t nV, nT, nExt, W, H;
+  uint32_t use_mv;
+  float maxEdge_in;          // the mesh's maxEdgeLength when !use_mv
+  uint32_t pix_base;         // first pixel of this job in the batch's pixel arenas
+};
+
+// Largest j with pref[j] <= g (pref[0] = 0, pref has n+1 entries, g < pref[n]).
+__device__ __forceinline__ uint32_t job_of(const uint32_t* __restrict__ pref, uint32_t n, uint32_t g) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(pref + mid) <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ float job_maxedge(const JobDev& J) {
+  return J.use_mv ? __uint_as_float(J.ctr->maxedge_bits) : J.maxEdge_in;
+}
+
+__global__ void init_jobs_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
+                                 uint32_t* __restrict__ queue) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j == 0) *queue = 0;
+  if (j >= njobs) return;
+  ViewCounters v;
+  v.nvis = 0; v.nrays = 0; v.nentries = 0; v.status = 0; v.steps = 0;
+  v.maxedge_bits = 0; v.pad = 0;
+  for (int k = 0; k < 4; ++k) { v.mm[k] = 0xffffffffu; v.mm[4 + k] = 0u; }
+  *jobs[j].ctr = v;
+}
+
+// ------------------------------------------------------------ view set-up
+
+// The view set-up kernels give each job a range of blocks (bpref: prefix of
+// blocks per job), so a block reduces within one job and ends with one
+// atomic per counter.
+
+__device__ __forceinline__ float warp_min(float v) {
+  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// rotateVolume (vfRayPreComp.cc:886-906) + the min/max normalizeVertices
+// needs, over the vertices of every job with a model-view.
+__global__ void __launch_bounds__(256) view_rotate_kernel(const JobDev* __restrict__ jobs,
+                                                          uint32_t njobs,
+                                                          const uint32_t* __restrict__ bpref) {
+  const uint32_t j = job_of(bpref, njobs, blockIdx.x);
+  const JobDev& J = jobs[j];
+  const uint32_t lb = blockIdx.x - bpref[j], nb = bpref[j + 1] - bpref[j];
+  const float4 rows[3] = {J.m0, J.m1, J.m2};
+  float mn[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+  float mx[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = lb * blockDim.x + threadIdx.x; i < J.nV; i += nb * blockDim.x) {
+    const float4 v = J.vert_in[i];
+    float r[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float acc = 0.0f;
+      acc = fadd(acc, fmul(rows[a].x, v.x));
+      acc = fadd(acc, fmul(rows[a].y, v.y));
+      acc = fadd(acc, fmul(rows[a].z, v.z));
+      acc = fadd(acc, fmul(rows[a].w, 1.0f));
+      r[a] = acc;
+    }
+    const float4 o = make_float4(r[0], r[1], r[2], v.w);
+    J.vview[i] = o;
+    const float c[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      mn[k] = fminf(mn[k], c[k]);
+      mx[k] = fmaxf(mx[k], c[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float a = warp_min(mn[k]), b = warp_max(mx[k]);
+    if ((threadIdx.x & 31u) == 0) {
+      atomicMin(&J.ctr->mm[k], f2ord(a));
+      atomicMax(&J.ctr->mm[4 + k], f2ord(b));
+    }
+  }
+}
+
+// normalizeVertices (vfRayPreComp.cc:84-145) with each view's min/max.
+__global__ void __launch_bounds__(256) view_normalize_kernel(const JobDev* __restrict__ jobs,
+                                                             uint32_t njobs,
+                                                             const uint32_t* __restrict__ bpref) {
+  const uint32_t j = job_of(bpref, njobs, blockIdx.x);
+  const JobDev& J = jobs[j];
+  const uint32_t lb = blockIdx.x - bpref[j], nb = bpref[j + 1] - bpref[j];
+  float mn[4], mx[4], cen[3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    mn[k] = ord2f(J.ctr->mm[k]);
+    mx[k] = ord2f(J.ctr->mm[4 + k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    cen[k] = (float)ddiv((double)fadd(mn[k], mx[k]), 2.0);
+    mx[k] = fsub(mx[k], cen[k]);
+    mn[k] = fsub(mn[k], cen[k]);
+  }
+  float maxCoord = (mx[1] > mx[2]) ? mx[1] : mx[2];
+  maxCoord = (mx[0] > maxCoord) ? mx[0] : maxCoord;
+  const float sc = (float)ddiv(1.0, (double)maxCoord);
+  const float ss = (float)ddiv(1.0, (double)fsub(mx[3], mn[3]));
+  for (uint32_t i = lb * blockDim.x + threadIdx.x; i < J.nV; i += nb * blockDim.x) {
+    float4 p = J.vview[i];
+    p.x = fmul(fsub(p.x, cen[0]), sc);
+    p.y = fmul(fsub(p.y, cen[1]), sc);
+    p.z = fmul(fsub(p.z, cen[2]), sc);
+    p.w = fmul(fsub(p.w, mn[3]), ss);
+    J.vview[i] = p;
+  }
+}
+
+// buildLmt's maxEdgeLength (vfRayPreComp.cc:810-836) over each view's vertices.
+__global__ void __launch_bounds__(256) view_maxedge_kernel(const JobDev* __restrict__ jobs,
+                                                           uint32_t njobs,
+                                                           const uint32_t* __restrict__ bpref) {
+  const uint32_t j = job_of(bpref, njobs, blockIdx.x);
+  const JobDev& J = jobs[j];
+  const uint32_t lb = blockIdx.x - bpref[j], nb = bpref[j + 1] - bpref[j];
+  float best = 0.0f;
+  for (uint32_t t = lb * blockDim.x + threadIdx.x; t < J.nT; t += nb * blockDim.x) {
+    const uint4 id = J.tet[t];
+    const float4 p[4] = {J.vview[id.x], J.vview[id.y], J.vview[id.z], J.vview[id.w]};
+    const int E[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float4 a = p[E[k][0]], b = p[E[k][1]];
+      const float e0 = fsub(a.x, b.x), e1 = fsub(a.y, b.y), e2 = fsub(a.z, b.z);
+      const float len = __fsqrt_rn(fadd(fadd(fmul(e0, e0), fmul(e1, e1)), fmul(e2, e2)));
+      if (len > best) best = len;
+    }
+  }
+  best = warp_max(best);
+  if ((threadIdx.x & 31u) == 0) atomicMax(&J.ctr->maxedge_bits, __float_as_uint(best));
+}
+
+// ------------------------------------------------------------ stage (a)
+
+// findVisibleFaces (vfRayKernelCPU.cc:51-132), one thread per external face;
+// each block of 1024 faces belongs to one job (bpref: blocks per job).
+__global__ void __launch_bounds__(1024) visible_kernel(const JobDev* __restrict__ jobs,
+                                                       uint32_t njobs,
+                                                       const uint32_t* __restrict__ bpref) {
+  const uint32_t j = job_of(bpref, njobs, blockIdx.x);
+  const JobDev& J = jobs[j];
+  const uint32_t lb = blockIdx.x - bpref[j];
+  const uint32_t e = lb * blockDim.x + threadIdx.x;
+  int vis = 0;
+  if (e < J.nExt) {
+    const uint2 tf = J.extf[e];
+    const uint4 id = J.tet[tf.x];
+    const float4 v0 = J.vert[sel4(id, tf.y & 3u)];
+    const float4 v1 = J.vert[sel4(id, (tf.y + 1) & 3u)];
+    const float4 v2 = J.vert[sel4(id, (tf.y + 2) & 3u)];
+    const float4 op = J.vert[sel4(id, (tf.y + 3) & 3u)];
+    Plane P;
+    face_plane(v0, v1, v2, P);
+    const float faceZ = plane_eval(op.x, op.y, P.zx, P.zy, P.zz);
+    if (faceZ < op.z) P.sx = -1.0f;  // :128 invisible sentinel
+    vis = (P.sx != -1.0f);
+    J.planes[2 * (size_t)e] = make_float4(P.zx, P.zy, P.zz, P.sx);
+    J.planes[2 * (size_t)e + 1] = make_float4(P.sy, P.sz, 0.0f, 0.0f);
+  }
+  const int cnt = __syncthreads_count(vis);
+  if (threadIdx.x == 0) J.blk[lb] = (uint32_t)cnt;
+}
+
+// Ordered compaction (main.cc:93-138, vfRay.cu:355-388): a block's offset is
+// the sum of the counts of the job's blocks before it; inside the block,
+// warp ballots and a warp-count prefix place each face at its rank.
+__global__ void __launch_bounds__(1024) compact_kernel(const JobDev* __restrict__ jobs,
+                                                       uint32_t njobs,
+                                                       const uint32_t* __restrict__ bpref) {
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_base;
+  const uint32_t j = job_of(bpref, njobs, blockIdx.x);
+  const JobDev& J = jobs[j];
+  const uint32_t lb = blockIdx.x - bpref[j];
+  const uint32_t nb = bpref[j + 1] - bpref[j];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t part = 0;
+  for (uint32_t b = threadIdx.x; b < lb; b += blockDim.x) part += J.blk[b];
+  for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  if (lane == 0) s_warp[warp] = part;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t x = s_warp[lane];
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) s_base = x;
+  }
+  __syncthreads();
+  const uint32_t e = lb * blockDim.x + threadIdx.x;
+  const bool vis = e < J.nExt && J.planes[2 * (size_t)e].w != -1.0f;
+  const uint32_t m = __ballot_sync(0xffffffffu, vis);
+  if (lane == 0) s_warp[warp] = __popc(m);
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t c = s_warp[lane];
+    uint32_t x = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    s_warp[lane] = x - c;
+    if (lb == nb - 1 && lane == 31) J.ctr->nvis = s_base + x;
+  }
+  __syncthreads();
+  if (vis) J.vis_ext[s_base + s_warp[warp] + __popc(m & ((1u << lane) - 1u))] = e;
+}
+
+// Exclusive prefix of a per-job device count (0: visible faces, 1: rays,
+// 2: entry-list entries) into out[0..njobs]; one block.
+__global__ void __launch_bounds__(1024) prefix_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
+                                                      int which, uint32_t* __restrict__ out) {
+  __shared__ uint32_t s[32];
+  __shared__ uint32_t s_carry;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < njobs; base += blockDim.x) {
+    const uint32_t j = base + threadIdx.x;
+    uint32_t v = 0;
+    if (j < njobs) {
+      const ViewCounters* c = jobs[j].ctr;
+      v = which == 0 ? c->nvis : (which == 1 ? c->nrays : c->nentries);
+    }
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t c = s[lane];
+      uint32_t z = c;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= (uint32_t)o) z += y;
+      }
+      s[lane] = z - c;
+    }
+    __syncthreads();
+    const uint32_t carry = s_carry;
+    if (j < njobs) out[j] = carry + s[warp] + x - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) s_carry = carry + s[warp] + x;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[njobs] = s_carry;
+}
+
+// ------------------------------------------------------------ stage (b)
+
+// projectVisibleFaces (vfRayKernelCPU.cc:136-169) + the pixel coverage of
+// vfRay's face loop (:248-274): persistent warps over the visible faces of
+// all jobs, one warp per face, one lane per bounding-box column, y ascending;
+// an out-of-range entry scalar ends the column (:274).  The reference lets
+// the last visible face in order write a pixel; visible order is ext-face
+// order, so the winner is the largest ext-face index reaching it: atomicMax.
+// Pixels outside the image are clipped (the reference would write past its
+// buffer there).  kCount/kFill: the composited mode's entry-list passes.
+template <bool kCount, bool kFill>
+__global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
+                                                     const uint32_t* __restrict__ vpref,
+                                                     uint2* __restrict__ ent, uint32_t ent_cap) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t total = vpref[njobs];
+  for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total; g += nwarps) {
+    const uint32_t j = job_of(vpref, njobs, g);
+    const JobDev& J = jobs[j];
+    const uint32_t i = g - vpref[j];
+    const uint32_t W = J.W, H = J.H;
+    const uint32_t e = J.vis_ext[i];
+    const uint2 tf = J.extf[e];
+    const uint4 id = J.tet[tf.x];
+    const float4 v0 = J.vert[sel4(id, tf.y & 3u)];
+    const float4 v1 = J.vert[sel4(id, (tf.y + 1) & 3u)];
+    const float4 v2 = J.vert[sel4(id, (tf.y + 2) & 3u)];
+    uint32_t bx = W - 1, by = H - 1, bz = 0, bw = 0;
+    const float4 vv[3] = {v0, v1, v2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t ix = to_pixel(vv[k].x, W), iy = to_pixel(vv[k].y, H);
+      if (ix < bx) bx = ix;
+      if (iy < by) by = iy;
+      if (ix > bz) bz = ix;
+      if (iy > bw) bw = iy;
+    }
+    if (!kFill && lane == 0) J.bbox[i] = make_uint4(bx, by, bz, bw);
+    const uint32_t xe = min(bz, W - 1), ye = min(bw, H - 1);
+    if (bx > xe || by > ye) continue;  // box entirely outside the image
+    const EntryEdges E = entry_edges(v0, v1, v2);
+    const float4 p0 = J.planes[2 * (size_t)e], p1 = J.planes[2 * (size_t)e + 1];
+    for (uint32_t px = bx + lane; px <= xe; px += 32) {
+      const float ox = obj_coord(px, W);
+      for (uint32_t py = by; py <= ye; ++py) {
+        const float oy = obj_coord(py, H);
+        if (!entry_inside(E, ox, oy)) continue;
+        const float sp = plane_eval(ox, oy, p0.w, p1.x, p1.y);
+        const uint32_t p = py * W + px;
+        if (kCount || kFill) {
+          if ((sp < 0.0f) || (sp > 1.0f)) continue;  // composited: only this pixel
+          if (kCount) {
+            atomicAdd(&J.ent_cnt[p], 1u);
+          } else {
+            const float zp = plane_eval(ox, oy, p0.x, p0.y, p0.z);
+            const uint32_t slot = J.ent_off[p] + atomicAdd(&J.ent_cur[p], 1u);
+            if (slot < ent_cap) ent[slot] = make_uint2(__float_as_uint(zp), e);
+          }
+        } else {
+          if ((sp < 0.0f) || (sp > 1.0f)) break;  // :274 rest of the column
+          atomicMax(&J.winner[p], (int32_t)e);
+        }
+      }
+    }
+  }
+}
+
+// Ray lists: the pixels with an entry face, in 8x4 screen tiles (one warp per
+// tile, tiles of all jobs in one index space) so that neighbouring rays,
+// which walk neighbouring tets, are neighbours in the list.  Pixels without
+// one are cleared in the outputs here (the reference zero-fills its image,
+// main.cc:194).
+__global__ void __launch_bounds__(256) raylist_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
+                                                      const uint32_t* __restrict__ tpref, int mode) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (g >= tpref[njobs]) return;
+  const uint32_t j = job_of(tpref, njobs, g);
+  const JobDev& J = jobs[j];
+  const uint32_t tile = g - tpref[j];
+  const uint32_t tx = (J.W + 7) >> 3;
+  const uint32_t x = (tile % tx) * 8 + (lane & 7), y = (tile / tx) * 4 + (lane >> 3);
+  bool has = false;
+  uint32_t p = 0;
+  const bool inside = x < J.W && y < J.H;
+  if (inside) {
+    p = y * J.W + x;
+    has = mode == 0 ? (J.winner[p] >= 0) : (J.ent_cnt[p] > 0);
+  }
+  const uint32_t m = __ballot_sync(0xffffffffu, has);
+  if (m) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&J.ctr->nrays, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (has) J.rays[base + __popc(m & ((1u << lane) - 1u))] = p;
+  }
+  if (inside && !has) {
+    if (J.rgb8) {
+      uint8_t* o = J.rgb8 + 3 * (size_t)p;
+      o[0] = 0; o[1] = 0; o[2] = 0;
+    }
+    if (J.rgba) J.rgba[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (J.steps) J.steps[p] = 0;
+  }
+}
+
+// Exclusive scan of the batch's entry-count arena (composited mode): block
+// scans, then each block adds the sums of the blocks before it.
+__global__ void __launch_bounds__(1024) scan_blocks_kernel(const uint32_t* __restrict__ in,
+                                                           uint32_t n, uint32_t* __restrict__ out,
+                                                           uint32_t* __restrict__ sums) {
+  __shared__ uint32_t s[32];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t v = i < n ? in[i] : 0u;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) s[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t c = s[lane];
+    uint32_t z = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+      if (lane >= (uint32_t)o) z += y;
+    }
+    s[lane] = z - c;
+    if (lane == 31) sums[blockIdx.x] = z;
+  }
+  __syncthreads();
+  if (i < n) out[i] = x - v + s[warp];
+}
+
+__global__ void __launch_bounds__(1024) scan_add_kernel(uint32_t* __restrict__ out, uint32_t n,
+                                                        const uint32_t* __restrict__ sums,
+                                                        uint32_t* __restrict__ total) {
+  __shared__ uint32_t s[32];
+  __shared__ uint32_t s_base;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t part = 0;
+  for (uint32_t b = threadIdx.x; b < blockIdx.x; b += blockDim.x) part += sums[b];
+  for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  if (lane == 0) s[warp] = part;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t x = s[lane];
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) s_base = x;
+  }
+  __syncthreads();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += s_base;
+  if (total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *total = s_base + sums[blockIdx.x];
+}
+
+// Per-job entry totals for the composited mode (for stats and overflow).
+__global__ void entry_totals_kernel(const JobDev* __restrict__ jobs, uint32_t njobs) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  const JobDev& J = jobs[j];
+  const uint32_t np = J.W * J.H;
+  J.ctr->nentries = J.ent_off[np] - J.ent_off[0];
+}
+
+}  // namespace vfr

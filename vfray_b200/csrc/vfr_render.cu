@@ -1,22 +1,23 @@
-// The C ABI of the VF-Ray render path (include/vfray.h): context, resident
-// meshes and tables, and the three stages of a view as stream-ordered launches.
+// The C ABI of the VF-Ray render path (include/vfray.h): contexts, resident
+// meshes and tables, and batches of views run as stream-ordered launches.
 //
 // Replaces the host driver of the reference (vfRay.cu:165-594): there the
 // stages communicate through globals, texture bindings and a host round trip
-// for the visible-face compaction; here a view is a chain of kernels on one
-// stream whose intermediate counts stay on the device, so a whole view can be
-// enqueued without a host synchronisation (and captured in a CUDA graph).
+// for the visible-face compaction; here a batch of views is one chain of
+// kernels on one stream whose intermediate counts stay on the device, so
+// nothing waits on the host between stages and the chain can be captured as a
+// CUDA graph.  A single view is a batch of one job.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
 #include <vector>
 
-#include "vfray.h"
-#include "vfr_kernels.cuh"
 #include "vfr_internal.h"
+#include "vfray.h"
 
 namespace vfr {
 
@@ -36,6 +37,22 @@ const char* status_string(int s) {
   }
 }
 
+// ------------------------------------------------------------------ Ctx
+
+Ctx::~Ctx() {
+  cudaStreamSynchronize(stream ? stream : own_stream);
+  meshes.clear();
+  if (d_tf) cudaFree(d_tf);
+  if (d_psi) cudaFree(d_psi);
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  for (auto* v : {&prof_pool, &prof_live})
+    for (auto& s : *v)
+      for (auto& e : s.e)
+        if (e) cudaEventDestroy(e);
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
 int Ctx::fail(int code, const std::string& msg) {
   err = msg;
   return code;
@@ -49,11 +66,15 @@ int Ctx::cuda(cudaError_t e, const char* what) {
 }
 
 int Ctx::grow(Buf& b, size_t bytes, const char* what) {
+  if (bytes == 0) bytes = 16;
   if (b.cap >= bytes && b.p) return VFR_OK;
-  if (b.p) cudaFree(b.p);
+  if (b.p) {
+    cudaStreamSynchronize(stream);  // in-flight work may still use the old buffer
+    cudaFree(b.p);
+  }
   b.p = nullptr;
   b.cap = 0;
-  size_t want = bytes + bytes / 8 + 256;
+  const size_t want = bytes + bytes / 8 + 256;
   int rc = cuda(cudaMalloc(&b.p, want), what);
   if (rc) return rc;
   b.cap = want;
@@ -63,142 +84,6 @@ int Ctx::grow(Buf& b, size_t bytes, const char* what) {
 Mesh* Ctx::mesh(int id) {
   if (id < 0 || id >= (int)meshes.size() || !meshes[id]) return nullptr;
   return meshes[id].get();
-}
-
-__global__ void init_counters_kernel(ViewCounters* c, uint32_t n) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  ViewCounters v;
-  v.nvis = 0; v.nrays = 0; v.queue = 0; v.status = 0; v.steps = 0; v.nentries = 0;
-  v.maxedge_bits = 0;
-  for (int k = 0; k < 4; ++k) { v.mm[k] = 0xffffffffu; v.mm[4 + k] = 0u; }
-  c[i] = v;
-}
-
-// Enqueue stage (a) (and the view set-up when mv16 is given).
-int Ctx::enqueue_visible(Mesh& m, const float* mv16, View& v) {
-  v.mesh = &m;
-  v.vert = m.vert;
-  v.use_view_maxedge = 0;
-  v.maxEdge = m.maxEdge;
-  init_counters_kernel<<<1, 32, 0, stream>>>(v.ctr, 1);
-  if (mv16) {
-    int rc = grow(v.vview, sizeof(float4) * (size_t)m.nV, "view vertices");
-    if (rc) return rc;
-    float4* vv = (float4*)v.vview.p;
-    const int blocks = std::max(1, std::min(num_sms * 4, (int)((m.nV + 255) / 256)));
-    view_rotate_kernel<<<blocks, 256, 0, stream>>>(
-        m.vert, m.nV, make_float4(mv16[0], mv16[1], mv16[2], mv16[3]),
-        make_float4(mv16[4], mv16[5], mv16[6], mv16[7]),
-        make_float4(mv16[8], mv16[9], mv16[10], mv16[11]), vv, v.ctr);
-    view_normalize_kernel<<<blocks, 256, 0, stream>>>(vv, m.nV, v.ctr);
-    const int tb = std::max(1, std::min(num_sms * 4, (int)((m.nT + 255) / 256)));
-    view_maxedge_kernel<<<tb, 256, 0, stream>>>(m.tet, vv, m.nT, v.ctr);
-    v.vert = vv;
-    v.use_view_maxedge = 1;
-  }
-  const uint32_t nblk = std::max<uint32_t>(1, (m.nExt + 1023) / 1024);
-  int rc = grow(v.planes, sizeof(float4) * 2 * (size_t)std::max<uint32_t>(m.nExt, 1), "planes");
-  if (!rc) rc = grow(v.blk, sizeof(uint32_t) * nblk, "block counts");
-  if (!rc) rc = grow(v.vis_ext, sizeof(uint32_t) * std::max<uint32_t>(m.nExt, 1), "visible list");
-  if (rc) return rc;
-  if (m.nExt) {
-    visible_kernel<<<nblk, 1024, 0, stream>>>(v.vert, m.tet, m.extf, m.nExt, (float4*)v.planes.p,
-                                             (uint32_t*)v.blk.p);
-    compact_kernel<<<nblk, 1024, 0, stream>>>((const float4*)v.planes.p, m.nExt,
-                                             (const uint32_t*)v.blk.p, (uint32_t*)v.vis_ext.p,
-                                             v.ctr);
-  }
-  return cuda(cudaGetLastError(), "stage (a) launch");
-}
-
-// Enqueue stage (b): coverage (winner or entry lists) + ray list.
-int Ctx::enqueue_project(View& v, uint32_t W, uint32_t H, int mode) {
-  Mesh& m = *v.mesh;
-  v.W = W; v.H = H; v.mode = mode;
-  const size_t np = (size_t)W * H;
-  int rc = grow(v.bbox, sizeof(uint4) * std::max<uint32_t>(m.nExt, 1), "bbox");
-  if (!rc) rc = grow(v.rays, sizeof(uint32_t) * np, "ray list");
-  if (rc) return rc;
-  const uint32_t warps = std::max<uint32_t>(8, std::min<uint32_t>(m.nExt, (uint32_t)num_sms * 64));
-  const uint32_t rb = (warps + 7) / 8;
-  const float4* planes = (const float4*)v.planes.p;
-  const uint32_t* vis = (const uint32_t*)v.vis_ext.p;
-  if (mode == VFR_MODE_REF) {
-    rc = grow(v.winner, sizeof(int32_t) * np, "winner map");
-    if (rc) return rc;
-    cudaMemsetAsync(v.winner.p, 0xff, sizeof(int32_t) * np, stream);
-    if (m.nExt)
-      raster_kernel<false, false><<<rb, 256, 0, stream>>>(
-          v.vert, m.tet, m.extf, planes, vis, v.ctr, W, H, (uint4*)v.bbox.p,
-          (int32_t*)v.winner.p, nullptr, nullptr, nullptr, nullptr, 0);
-  } else {
-    const uint32_t nsb = (uint32_t)((np + 1 + 1023) / 1024);
-    rc = grow(v.ent_cnt, sizeof(uint32_t) * (np + 1), "entry counts");
-    if (!rc) rc = grow(v.ent_off, sizeof(uint32_t) * (np + 1), "entry offsets");
-    if (!rc) rc = grow(v.ent_cur, sizeof(uint32_t) * np, "entry cursors");
-    if (!rc) rc = grow(v.scan, sizeof(uint32_t) * nsb, "scan sums");
-    if (!rc) rc = grow(v.ent, sizeof(uint2) * std::max<size_t>(v.ent_cap, 1), "entries");
-    if (rc) return rc;
-    cudaMemsetAsync(v.ent_cnt.p, 0, sizeof(uint32_t) * (np + 1), stream);
-    cudaMemsetAsync(v.ent_cur.p, 0, sizeof(uint32_t) * np, stream);
-    if (m.nExt)
-      raster_kernel<true, false><<<rb, 256, 0, stream>>>(
-          v.vert, m.tet, m.extf, planes, vis, v.ctr, W, H, (uint4*)v.bbox.p, nullptr,
-          (uint32_t*)v.ent_cnt.p, nullptr, nullptr, nullptr, 0);
-    scan_blocks_kernel<<<nsb, 1024, 0, stream>>>((const uint32_t*)v.ent_cnt.p, (uint32_t)(np + 1),
-                                                 (uint32_t*)v.ent_off.p, (uint32_t*)v.scan.p);
-    scan_add_kernel<<<nsb, 1024, 0, stream>>>((uint32_t*)v.ent_off.p, (uint32_t)(np + 1),
-                                              (const uint32_t*)v.scan.p, &v.ctr->nentries);
-    if (m.nExt)
-      raster_kernel<false, true><<<rb, 256, 0, stream>>>(
-          v.vert, m.tet, m.extf, planes, vis, v.ctr, W, H, nullptr, nullptr, nullptr,
-          (const uint32_t*)v.ent_off.p, (uint32_t*)v.ent_cur.p, (uint2*)v.ent.p,
-          (uint32_t)std::min<size_t>(v.ent_cap, 0xffffffffu));
-  }
-  const uint32_t tiles = ((W + 7) / 8) * ((H + 3) / 4);
-  raylist_kernel<<<(tiles + 7) / 8, 256, 0, stream>>>(
-      mode == VFR_MODE_REF ? (const int32_t*)v.winner.p : nullptr,
-      mode == VFR_MODE_REF ? nullptr : (const uint32_t*)v.ent_cnt.p, W, H, (uint32_t*)v.rays.p,
-      v.ctr);
-  return cuda(cudaGetLastError(), "stage (b) launch");
-}
-
-// Enqueue stage (c) into the given output buffers (device pointers).
-int Ctx::enqueue_traverse(View& v, uint8_t* rgb8, float4* rgba, uint32_t* steps) {
-  Mesh& m = *v.mesh;
-  const size_t np = (size_t)v.W * v.H;
-  if (rgb8) cudaMemsetAsync(rgb8, 0, np * 3, stream);
-  if (rgba) cudaMemsetAsync(rgba, 0, np * sizeof(float4), stream);
-  if (steps) cudaMemsetAsync(steps, 0, np * sizeof(uint32_t), stream);
-  TraverseParams P;
-  P.tet = m.tet; P.walk = m.walk; P.vert = v.vert; P.extf = m.extf;
-  P.planes = (const float4*)v.planes.p;
-  P.winner = (const int32_t*)v.winner.p;
-  P.rays = (const uint32_t*)v.rays.p;
-  P.ent_off = (const uint32_t*)v.ent_off.p;
-  P.ent = (const uint2*)v.ent.p;
-  P.ctr = v.ctr;
-  P.tf = d_tf; P.psi = d_psi;
-  P.rgb8 = rgb8; P.rgba = rgba; P.steps = steps;
-  P.W = v.W; P.H = v.H; P.nT = m.nT; P.nV = m.nV;
-  P.maxEdge = v.maxEdge;
-  P.use_view_maxedge = v.use_view_maxedge;
-  P.step_cap = step_cap ? step_cap : (uint32_t)std::min<uint64_t>(4ull * m.nT + 64, 0x7fffffffull);
-  P.chunk = tune.chunk;
-  P.refill = tune.refill;
-  P.psi_one = psi_one ? 1u : 0u;
-  P.ent_cap = (uint32_t)std::min<size_t>(v.ent_cap, 0xffffffffu);
-  const int blocks = num_sms * traverse_blocks_per_sm(v.mode);
-  const void* fn = traverse_fn(v.mode, tune.variant);
-  void* args[] = {&P};
-  return cuda(cudaLaunchKernel(fn, dim3(blocks), dim3(256), args, 0, stream), "stage (c) launch");
-}
-
-const void* Ctx::traverse_fn(int mode, uint32_t variant) {
-  if (mode == VFR_MODE_REF)
-    return variant ? (const void*)traverse_kernel<0, 3> : (const void*)traverse_kernel<0, 2>;
-  return variant ? (const void*)traverse_kernel<1, 3> : (const void*)traverse_kernel<1, 2>;
 }
 
 void Ctx::prof_mark(int k) {
@@ -216,6 +101,12 @@ void Ctx::prof_mark(int k) {
   cudaEventRecord(prof_live.back().e[k], stream);
 }
 
+const void* Ctx::traverse_fn(int mode, uint32_t variant) {
+  if (mode == VFR_MODE_REF)
+    return variant ? (const void*)traverse_kernel<0, 3> : (const void*)traverse_kernel<0, 2>;
+  return variant ? (const void*)traverse_kernel<1, 3> : (const void*)traverse_kernel<1, 2>;
+}
+
 int Ctx::traverse_blocks_per_sm(int mode) {
   if (tune.blocks_per_sm) return (int)tune.blocks_per_sm;
   int& cached = occ[(mode ? 2 : 0) + (tune.variant ? 1 : 0)];
@@ -227,38 +118,357 @@ int Ctx::traverse_blocks_per_sm(int mode) {
   return cached;
 }
 
-int Ctx::read_counters(View& v, ViewCounters& out) {
-  int rc = cuda(cudaMemcpyAsync(h_ctr, v.ctr, sizeof(ViewCounters), cudaMemcpyDeviceToHost, stream),
-                "counter read");
-  if (!rc) rc = cuda(cudaStreamSynchronize(stream), "stream sync");
-  if (!rc) out = *h_ctr;
-  return rc;
-}
-
-int Ctx::check_status(const ViewCounters& c) {
-  if (c.status & (VFR_DEV_ABANDON | VFR_DEV_RANGE | VFR_DEV_STEP_CAP | VFR_DEV_OVERFLOW)) {
+int Ctx::check_status(uint32_t status, uint32_t overflow) {
+  if (overflow) return fail(VFR_ERR_DEVICE, "entry lists overflowed; render again");
+  if (status & (VFR_DEV_ABANDON | VFR_DEV_RANGE | VFR_DEV_STEP_CAP | VFR_DEV_OVERFLOW)) {
     char buf[128];
     std::snprintf(buf, sizeof buf, "device status 0x%x (abandon=1 step-cap=2 range=4 overflow=16)",
-                  c.status);
+                  status);
     return fail(VFR_ERR_DEVICE, buf);
   }
   return VFR_OK;
 }
 
+// ------------------------------------------------------------------ Batch
+
+Batch::~Batch() {
+  drop_graph();
+  if (stage) cudaFreeHost(stage);
+  if (stage_done) cudaEventDestroy(stage_done);
+}
+
+void Batch::drop_graph() {
+  if (exec) cudaGraphExecDestroy(exec);
+  exec = nullptr;
+}
+
+static uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// Lays the jobs out in the batch's arenas (allocating what is missing) and
+// fills the job table on the host.
+int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
+  Ctx& C = *ctx;
+  specs = s;
+  mode = m;
+  njobs = (uint32_t)s.size();
+  jobs.assign(njobs, JobDev{});
+  pref.assign(4 * (size_t)(njobs + 1), 0);
+  uint32_t* pr = pref.data();
+  uint32_t* pe = pr + (njobs + 1);
+  uint32_t* px = pe + (njobs + 1);
+  uint32_t* pt = px + (njobs + 1);
+  size_t nv_mv = 0, next = 0, nblk = 0, pix = 0;
+  for (uint32_t j = 0; j < njobs; ++j) {
+    Mesh* mesh = C.mesh(s[j].mesh);
+    if (!mesh) return C.fail(VFR_ERR_STATE, "unknown mesh id in job");
+    const JobSpec& q = s[j];
+    if (q.W < 2 || q.H < 2 || (uint64_t)q.W * q.H > (1ull << 28))
+      return C.fail(VFR_ERR_INVALID, "image size out of range");
+    const uint32_t rb =
+        q.use_mv ? std::max<uint32_t>(1, std::min<uint32_t>(cdiv(mesh->nV, 1024), 2 * C.num_sms)) : 0;
+    const uint32_t eb =
+        q.use_mv ? std::max<uint32_t>(1, std::min<uint32_t>(cdiv(mesh->nT, 1024), 4 * C.num_sms)) : 0;
+    const uint32_t xb = cdiv(mesh->nExt, 1024);
+    const uint32_t tl = cdiv(q.W, 8) * cdiv(q.H, 4);
+    pr[j + 1] = pr[j] + rb;
+    pe[j + 1] = pe[j] + eb;
+    px[j + 1] = px[j] + xb;
+    pt[j + 1] = pt[j] + tl;
+    nv_mv += q.use_mv ? mesh->nV : 0;
+    next += mesh->nExt;
+    nblk += xb;
+    pix += (size_t)q.W * q.H;
+  }
+  rot_blocks = pr[njobs];
+  edge_blocks = pe[njobs];
+  ext_blocks = px[njobs];
+  tiles = pt[njobs];
+  pixels = pix;
+  ext_total = next;
+  if (pix > 0xffffffffull || next > 0xffffffffull) return C.fail(VFR_ERR_BUDGET, "batch too large");
+  const size_t old_sig = (size_t)vview.p ^ (size_t)planes.p ^ (size_t)winner.p ^ (size_t)rays.p ^
+                         (size_t)ent.p ^ (size_t)d_jobs.p;
+  int rc = C.grow(d_jobs, sizeof(JobDev) * njobs, "job table");
+  if (!rc) rc = C.grow(d_pref, sizeof(uint32_t) * pref.size(), "job prefixes");
+  if (!rc) rc = C.grow(d_dev_pref, sizeof(uint32_t) * (2 * (size_t)(njobs + 1) + 4), "device prefixes");
+  if (!rc) rc = C.grow(d_ctr, sizeof(ViewCounters) * njobs, "view counters");
+  if (!rc) rc = C.grow(vview, sizeof(float4) * nv_mv, "view vertices");
+  if (!rc) rc = C.grow(planes, sizeof(float4) * 2 * next, "planes");
+  if (!rc) rc = C.grow(blk, sizeof(uint32_t) * nblk, "block counts");
+  if (!rc) rc = C.grow(vis, sizeof(uint32_t) * next, "visible lists");
+  if (!rc) rc = C.grow(bbox, sizeof(uint4) * next, "bboxes");
+  if (!rc) rc = C.grow(rays, sizeof(uint32_t) * pix, "ray lists");
+  if (!rc && mode == VFR_MODE_REF) rc = C.grow(winner, sizeof(int32_t) * pix, "winner maps");
+  if (!rc && mode == VFR_MODE_COMPOSITED) {
+    if (ent_cap == 0) ent_cap = C.ent_cap_hint ? C.ent_cap_hint : pix * 4 + 1024;
+    rc = C.grow(ent_cnt, sizeof(uint32_t) * (pix + 1), "entry counts");
+    if (!rc) rc = C.grow(ent_off, sizeof(uint32_t) * (pix + 1), "entry offsets");
+    if (!rc) rc = C.grow(ent_cur, sizeof(uint32_t) * pix, "entry cursors");
+    if (!rc) rc = C.grow(scan, sizeof(uint32_t) * (cdiv(pix + 1, 1024) + 1), "scan sums");
+    if (!rc) rc = C.grow(ent, sizeof(uint2) * ent_cap, "entries");
+  }
+  if (!rc && own_outputs) {
+    rc = C.grow(out_rgb8, 3 * pix, "rgb8 outputs");
+    if (!rc) rc = C.grow(out_rgba, sizeof(float4) * pix, "rgba outputs");
+    if (!rc) rc = C.grow(out_steps, sizeof(uint32_t) * pix, "steps outputs");
+  }
+  if (rc) return rc;
+  const size_t new_sig = (size_t)vview.p ^ (size_t)planes.p ^ (size_t)winner.p ^ (size_t)rays.p ^
+                         (size_t)ent.p ^ (size_t)d_jobs.p;
+  if (new_sig != old_sig) drop_graph();
+  scratch_bytes = vview.cap + planes.cap + blk.cap + vis.cap + bbox.cap + rays.cap + winner.cap +
+                  ent_cnt.cap + ent_off.cap + ent_cur.cap + ent.cap + scan.cap + d_ctr.cap;
+  size_t ov = 0, oe = 0, ob = 0, op = 0;
+  for (uint32_t j = 0; j < njobs; ++j) {
+    Mesh* mesh = C.mesh(s[j].mesh);
+    const JobSpec& q = s[j];
+    JobDev& J = jobs[j];
+    J.m0 = make_float4(q.mv[0], q.mv[1], q.mv[2], q.mv[3]);
+    J.m1 = make_float4(q.mv[4], q.mv[5], q.mv[6], q.mv[7]);
+    J.m2 = make_float4(q.mv[8], q.mv[9], q.mv[10], q.mv[11]);
+    J.tet = mesh->tet;
+    J.walk = mesh->walk;
+    J.vert_in = mesh->vert;
+    J.extf = mesh->extf;
+    J.vview = q.use_mv ? vview.as<float4>(sizeof(float4) * ov) : nullptr;
+    J.vert = q.use_mv ? J.vview : mesh->vert;
+    J.planes = planes.as<float4>(sizeof(float4) * 2 * oe);
+    J.blk = blk.as<uint32_t>(sizeof(uint32_t) * ob);
+    J.vis_ext = vis.as<uint32_t>(sizeof(uint32_t) * oe);
+    J.bbox = bbox.as<uint4>(sizeof(uint4) * oe);
+    J.winner = mode == VFR_MODE_REF ? winner.as<int32_t>(sizeof(int32_t) * op) : nullptr;
+    J.rays = rays.as<uint32_t>(sizeof(uint32_t) * op);
+    J.ent_cnt = mode == VFR_MODE_COMPOSITED ? ent_cnt.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
+    J.ent_off = mode == VFR_MODE_COMPOSITED ? ent_off.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
+    J.ent_cur = mode == VFR_MODE_COMPOSITED ? ent_cur.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
+    J.ctr = d_ctr.as<ViewCounters>(sizeof(ViewCounters) * j);
+    if (own_outputs) {
+      specs[j].rgb8 = out_rgb8.as<uint8_t>(3 * op);
+      specs[j].rgba = out_rgba.as<float4>(sizeof(float4) * op);
+      specs[j].steps = out_steps.as<uint32_t>(sizeof(uint32_t) * op);
+    }
+    J.rgb8 = specs[j].rgb8;
+    J.rgba = specs[j].rgba;
+    J.steps = specs[j].steps;
+    J.nV = mesh->nV;
+    J.nT = mesh->nT;
+    J.nExt = mesh->nExt;
+    J.W = q.W;
+    J.H = q.H;
+    J.use_mv = q.use_mv ? 1u : 0u;
+    J.maxEdge_in = mesh->maxEdge;
+    J.pix_base = (uint32_t)op;
+    ov += q.use_mv ? mesh->nV : 0;
+    oe += mesh->nExt;
+    ob += cdiv(mesh->nExt, 1024);
+    op += (size_t)q.W * q.H;
+  }
+  return VFR_OK;
+}
+
+// Uploads the job table and prefixes; async: through pinned staging, stream
+// ordered (the staging is reused only after the previous copy has run).
+int Batch::upload(bool async) {
+  Ctx& C = *ctx;
+  const size_t bj = sizeof(JobDev) * njobs, bp = sizeof(uint32_t) * pref.size();
+  if (!async) {
+    int rc = C.cuda(cudaMemcpyAsync(d_jobs.p, jobs.data(), bj, cudaMemcpyHostToDevice, C.stream),
+                    "job table upload");
+    if (!rc)
+      rc = C.cuda(cudaMemcpyAsync(d_pref.p, pref.data(), bp, cudaMemcpyHostToDevice, C.stream),
+                  "prefix upload");
+    if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "upload");
+    return rc;
+  }
+  if (!stage_done) cudaEventCreateWithFlags(&stage_done, cudaEventDisableTiming);
+  if (stage_cap < bj + bp) {
+    cudaEventSynchronize(stage_done);
+    if (stage) cudaFreeHost(stage);
+    stage = nullptr;
+    stage_cap = 0;
+    if (cudaMallocHost(&stage, bj + bp + 4096) != cudaSuccess) return C.fail(VFR_ERR_NOMEM, "staging");
+    stage_cap = bj + bp + 4096;
+  }
+  cudaEventSynchronize(stage_done);
+  std::memcpy(stage, jobs.data(), bj);
+  std::memcpy((char*)stage + bj, pref.data(), bp);
+  int rc = C.cuda(cudaMemcpyAsync(d_jobs.p, stage, bj, cudaMemcpyHostToDevice, C.stream),
+                  "job table upload");
+  if (!rc)
+    rc = C.cuda(cudaMemcpyAsync(d_pref.p, (char*)stage + bj, bp, cudaMemcpyHostToDevice, C.stream),
+                "prefix upload");
+  cudaEventRecord(stage_done, C.stream);
+  return rc;
+}
+
+int Batch::enqueue_a() {
+  Ctx& C = *ctx;
+  cudaStream_t st = C.stream;
+  const JobDev* J = d_jobs.as<JobDev>();
+  const uint32_t* P = d_pref.as<uint32_t>();
+  const uint32_t n1 = njobs + 1;
+  init_jobs_kernel<<<cdiv(njobs, 128), 128, 0, st>>>(J, njobs, queue());
+  if (rot_blocks) {
+    view_rotate_kernel<<<rot_blocks, 256, 0, st>>>(J, njobs, P);
+    view_normalize_kernel<<<rot_blocks, 256, 0, st>>>(J, njobs, P);
+    view_maxedge_kernel<<<edge_blocks, 256, 0, st>>>(J, njobs, P + n1);
+  }
+  if (ext_blocks) {
+    visible_kernel<<<ext_blocks, 1024, 0, st>>>(J, njobs, P + 2 * n1);
+    compact_kernel<<<ext_blocks, 1024, 0, st>>>(J, njobs, P + 2 * n1);
+  }
+  prefix_kernel<<<1, 1024, 0, st>>>(J, njobs, 0, vis_pref());
+  return C.cuda(cudaGetLastError(), "stage (a) launch");
+}
+
+int Batch::enqueue_b() {
+  Ctx& C = *ctx;
+  cudaStream_t st = C.stream;
+  const JobDev* J = d_jobs.as<JobDev>();
+  const uint32_t* P = d_pref.as<uint32_t>();
+  const uint32_t n1 = njobs + 1;
+  const uint32_t rb = std::max(1, C.num_sms * (int)C.tune.raster_warps_per_sm / 8);
+  if (mode == VFR_MODE_REF) {
+    cudaMemsetAsync(winner.p, 0xff, sizeof(int32_t) * pixels, st);
+    raster_kernel<false, false><<<rb, 256, 0, st>>>(J, njobs, vis_pref(), nullptr, 0);
+  } else {
+    const uint32_t n = (uint32_t)pixels + 1, nsb = cdiv(n, 1024);
+    cudaMemsetAsync(ent_cnt.p, 0, sizeof(uint32_t) * n, st);
+    cudaMemsetAsync(ent_cur.p, 0, sizeof(uint32_t) * pixels, st);
+    raster_kernel<true, false><<<rb, 256, 0, st>>>(J, njobs, vis_pref(), nullptr, 0);
+    scan_blocks_kernel<<<nsb, 1024, 0, st>>>(ent_cnt.as<uint32_t>(), n, ent_off.as<uint32_t>(),
+                                             scan.as<uint32_t>());
+    scan_add_kernel<<<nsb, 1024, 0, st>>>(ent_off.as<uint32_t>(), n, scan.as<uint32_t>(), nullptr);
+    raster_kernel<false, true><<<rb, 256, 0, st>>>(J, njobs, vis_pref(), ent.as<uint2>(),
+                                                   (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu));
+    entry_totals_kernel<<<cdiv(njobs, 128), 128, 0, st>>>(J, njobs);
+  }
+  if (tiles) raylist_kernel<<<cdiv(tiles, 8), 256, 0, st>>>(J, njobs, P + 3 * n1, mode);
+  prefix_kernel<<<1, 1024, 0, st>>>(J, njobs, 1, ray_pref());
+  return C.cuda(cudaGetLastError(), "stage (b) launch");
+}
+
+int Batch::enqueue_c() {
+  Ctx& C = *ctx;
+  TraverseParams P;
+  P.jobs = d_jobs.as<JobDev>();
+  P.njobs = njobs;
+  P.ray_pref = ray_pref();
+  P.queue = queue();
+  P.ent = mode == VFR_MODE_COMPOSITED ? ent.as<uint2>() : nullptr;
+  P.ent_cap = (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu);
+  P.tf = C.d_tf;
+  P.psi = C.d_psi;
+  P.psi_one = C.psi_one ? 1u : 0u;
+  P.step_cap = C.step_cap;
+  P.refill = C.tune.refill;
+  const int blocks = C.num_sms * C.traverse_blocks_per_sm(mode);
+  void* args[] = {&P};
+  return C.cuda(cudaLaunchKernel(C.traverse_fn(mode, C.tune.variant), dim3(blocks), dim3(256), args,
+                                 0, C.stream),
+                "stage (c) launch");
+}
+
+int Batch::capture() {
+  Ctx& C = *ctx;
+  drop_graph();
+  cudaGraph_t g = nullptr;
+  int rc = C.cuda(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal), "capture");
+  if (rc) return rc;
+  rc = enqueue_all();
+  cudaError_t e = cudaStreamEndCapture(C.stream, &g);
+  if (!rc) rc = C.cuda(e, "end capture");
+  if (!rc) rc = C.cuda(cudaGraphInstantiate(&exec, g, 0), "graph instantiate");
+  if (g) cudaGraphDestroy(g);
+  if (rc) exec = nullptr;
+  return rc;
+}
+
+int Batch::run() {
+  if (exec) return ctx->cuda(cudaGraphLaunch(exec, ctx->stream), "graph launch");
+  return enqueue_all();
+}
+
+int Batch::counters(std::vector<ViewCounters>& out) {
+  Ctx& C = *ctx;
+  out.resize(njobs);
+  int rc = C.cuda(cudaMemcpyAsync(out.data(), d_ctr.p, sizeof(ViewCounters) * njobs,
+                                  cudaMemcpyDeviceToHost, C.stream),
+                  "counter read");
+  if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "stream sync");
+  return rc;
+}
+
 }  // namespace vfr
 
+using vfr::Batch;
 using vfr::Ctx;
+using vfr::JobSpec;
 using vfr::Mesh;
 
 struct vfr_ctx {
   Ctx impl;
 };
 
-#define CTX_OR_FAIL(c)                  \
-  if (!(c)) return VFR_ERR_INVALID;     \
-  Ctx& C = (c)->impl;                   \
-  (void)C;                              \
+struct vfr_batch {
+  vfr_ctx* owner = nullptr;
+  Batch b;
+};
+
+#define CTX_OR_FAIL(c)              \
+  if (!(c)) return VFR_ERR_INVALID; \
+  Ctx& C = (c)->impl;               \
+  (void)C;                          \
   cudaSetDevice(C.device);
+
+namespace {
+
+void fill_stats(const vfr::ViewCounters& k, uint32_t next, vfr_render_stats* s) {
+  s->num_ext = next;
+  s->num_vis = k.nvis;
+  s->num_rays = k.nrays;
+  s->num_entries = k.nentries;
+  s->num_steps = k.steps;
+  s->device_status = k.status;
+}
+
+// The single-view calls run the context's one-job batch.
+int single(Ctx& C, int mesh, const float* mv16, uint32_t W, uint32_t H, int mode, bool own,
+           uint8_t* rgb8, float4* rgba, uint32_t* steps) {
+  JobSpec q;
+  q.mesh = mesh;
+  q.W = W;
+  q.H = H;
+  q.use_mv = mv16 != nullptr;
+  if (mv16) std::memcpy(q.mv, mv16, sizeof q.mv);
+  q.rgb8 = rgb8;
+  q.rgba = rgba;
+  q.steps = steps;
+  C.plain.ctx = &C;
+  int rc = C.plain.layout({q}, mode, own);
+  if (!rc) rc = C.plain.upload(true);
+  return rc;
+}
+
+int copy_out(Ctx& C, uint8_t* rgb8, float* rgba, uint32_t* steps, size_t np) {
+  Batch& B = C.plain;
+  int rc = VFR_OK;
+  if (rgb8)
+    rc = C.cuda(cudaMemcpyAsync(rgb8, B.out_rgb8.p, np * 3, cudaMemcpyDeviceToHost, C.stream),
+                "rgb8 read");
+  if (!rc && rgba)
+    rc = C.cuda(cudaMemcpyAsync(rgba, B.out_rgba.p, np * sizeof(float4), cudaMemcpyDeviceToHost,
+                                C.stream),
+                "rgba read");
+  if (!rc && steps)
+    rc = C.cuda(cudaMemcpyAsync(steps, B.out_steps.p, np * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, C.stream),
+                "steps read");
+  if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "output read");
+  return rc;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -280,8 +490,7 @@ int vfr_create(vfr_ctx** out, int device) {
   if (cudaStreamCreateWithFlags(&C.own_stream, cudaStreamNonBlocking) != cudaSuccess)
     return VFR_ERR_CUDA;
   C.stream = C.own_stream;
-  if (cudaMallocHost(&C.h_ctr, sizeof(vfr::ViewCounters)) != cudaSuccess) return VFR_ERR_NOMEM;
-  if (cudaMalloc(&C.view.ctr, sizeof(vfr::ViewCounters)) != cudaSuccess) return VFR_ERR_NOMEM;
+  C.plain.ctx = &C;
   for (auto& e : C.ev) cudaEventCreate(&e);
   *out = c.release();
   return VFR_OK;
@@ -291,6 +500,13 @@ void vfr_destroy(vfr_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->impl.device);
   cudaStreamSynchronize(c->impl.stream);
+  // batches that outlive their context keep only their own memory; any call
+  // on them but vfr_batch_destroy then returns VFR_ERR_STATE
+  for (void* p : c->impl.batches) {
+    vfr_batch* b = static_cast<vfr_batch*>(p);
+    b->owner = nullptr;
+    b->b.ctx = nullptr;
+  }
   delete c;
 }
 
@@ -298,7 +514,9 @@ const char* vfr_last_error(const vfr_ctx* c) { return c ? c->impl.err.c_str() : 
 
 int vfr_set_stream(vfr_ctx* c, void* stream) {
   CTX_OR_FAIL(c);
+  cudaStreamSynchronize(C.stream);
   C.stream = stream ? (cudaStream_t)stream : C.own_stream;
+  C.plain.drop_graph();
   return VFR_OK;
 }
 
@@ -314,8 +532,7 @@ int vfr_set_option(vfr_ctx* c, int option, int64_t value) {
     case VFR_OPT_STEP_CAP: C.step_cap = (uint32_t)value; return VFR_OK;
     case VFR_OPT_QUEUE_CHUNK:
       if (value < 1) return C.fail(VFR_ERR_INVALID, "queue chunk must be >= 1");
-      C.tune.chunk = (uint32_t)value;
-      return VFR_OK;
+      return VFR_OK;  // kept for the ABI: the refill kernel takes one ray per lane
     case VFR_OPT_BLOCKS_PER_SM: C.tune.blocks_per_sm = (uint32_t)value; return VFR_OK;
     case VFR_OPT_PROFILE: C.profile = value != 0; return VFR_OK;
     case VFR_OPT_TRAVERSE_VARIANT:
@@ -325,6 +542,10 @@ int vfr_set_option(vfr_ctx* c, int option, int64_t value) {
     case VFR_OPT_REFILL:
       if (value < 1 || value > 32) return C.fail(VFR_ERR_INVALID, "refill is 1..32");
       C.tune.refill = (uint32_t)value;
+      return VFR_OK;
+    case VFR_OPT_RASTER_WARPS:
+      if (value < 1 || value > 64) return C.fail(VFR_ERR_INVALID, "raster warps per SM is 1..64");
+      C.tune.raster_warps_per_sm = (uint32_t)value;
       return VFR_OK;
     default: return C.fail(VFR_ERR_INVALID, "unknown option");
   }
@@ -362,14 +583,12 @@ int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
     if (!rc) rc = C.cuda(cudaMalloc(&C.d_psi, sizeof(float) * 512 * 512), "psi alloc");
     if (rc) return rc;
   }
+  cudaStreamSynchronize(C.stream);
   C.psi_one = psi[0] == 1.0f;
-  int rc = C.cuda(cudaMemcpyAsync(C.d_tf, tf, sizeof(float) * 1024, cudaMemcpyHostToDevice, C.stream),
-                  "tf upload");
+  int rc = C.cuda(cudaMemcpy(C.d_tf, tf, sizeof(float) * 1024, cudaMemcpyHostToDevice), "tf upload");
   if (!rc)
-    rc = C.cuda(cudaMemcpyAsync(C.d_psi, psi, sizeof(float) * 512 * 512, cudaMemcpyHostToDevice,
-                                C.stream),
+    rc = C.cuda(cudaMemcpy(C.d_psi, psi, sizeof(float) * 512 * 512, cudaMemcpyHostToDevice),
                 "psi upload");
-  if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "table upload");
   return rc;
 }
 
@@ -385,8 +604,12 @@ int vfr_mesh_upload(vfr_ctx* c, const float* vert4, uint32_t nV, const uint32_t*
   std::vector<uint32_t> walk(8 * (size_t)nT);
   if (!vfr::build_walk(tet4, con4, nV, nT, walk.data(), why)) return C.fail(VFR_ERR_MESH, why);
   std::unique_ptr<Mesh> m(new Mesh);
-  m->nV = nV; m->nT = nT; m->nExt = nExt;
-  m->maxEdge = maxEdge; m->maxZ = maxZ; m->minZ = minZ;
+  m->nV = nV;
+  m->nT = nT;
+  m->nExt = nExt;
+  m->maxEdge = maxEdge;
+  m->maxZ = maxZ;
+  m->minZ = minZ;
   int rc = C.cuda(cudaMalloc(&m->tet, sizeof(uint4) * (size_t)nT), "tets");
   if (!rc) rc = C.cuda(cudaMalloc(&m->walk, sizeof(vfr::WalkRec) * (size_t)nT), "walk records");
   if (!rc) rc = C.cuda(cudaMalloc(&m->vert, sizeof(float4) * (size_t)nV), "vertices");
@@ -422,7 +645,10 @@ int vfr_mesh_release(vfr_ctx* c, int id) {
   CTX_OR_FAIL(c);
   if (!C.mesh(id)) return C.fail(VFR_ERR_STATE, "unknown mesh id");
   cudaStreamSynchronize(C.stream);
-  if (C.view.mesh == C.mesh(id)) { C.view.mesh = nullptr; C.view.stage = 0; }
+  if (C.plain.njobs && C.plain.specs[0].mesh == id) {
+    C.plain.njobs = 0;
+    C.stage = 0;
+  }
   C.meshes[id].reset();
   return VFR_OK;
 }
@@ -439,20 +665,20 @@ int vfr_find_visible(vfr_ctx* c, int id, uint32_t* num_vis, uint32_t* visExt, fl
   CTX_OR_FAIL(c);
   Mesh* m = C.mesh(id);
   if (!m) return C.fail(VFR_ERR_STATE, "unknown mesh id");
-  C.view.stage = 0;
-  int rc = C.enqueue_visible(*m, nullptr, C.view);
-  vfr::ViewCounters k;
-  if (!rc) rc = C.read_counters(C.view, k);
+  C.stage = 0;
+  int rc = single(C, id, nullptr, 2, 2, VFR_MODE_REF, true, nullptr, nullptr, nullptr);
+  if (!rc) rc = C.plain.enqueue_a();
+  std::vector<vfr::ViewCounters> k;
+  if (!rc) rc = C.plain.counters(k);
   if (rc) return rc;
-  if (num_vis) *num_vis = k.nvis;
-  if (visExt && k.nvis)
-    rc = C.cuda(cudaMemcpy(visExt, C.view.vis_ext.p, sizeof(uint32_t) * k.nvis,
-                           cudaMemcpyDeviceToHost),
+  if (num_vis) *num_vis = k[0].nvis;
+  const vfr::JobDev& J = C.plain.jobs[0];
+  if (visExt && k[0].nvis)
+    rc = C.cuda(cudaMemcpy(visExt, J.vis_ext, sizeof(uint32_t) * k[0].nvis, cudaMemcpyDeviceToHost),
                 "visible list read");
   if (!rc && faceData && m->nExt) {
     std::vector<float4> pl(2 * (size_t)m->nExt);
-    rc = C.cuda(cudaMemcpy(pl.data(), C.view.planes.p, sizeof(float4) * pl.size(),
-                           cudaMemcpyDeviceToHost),
+    rc = C.cuda(cudaMemcpy(pl.data(), J.planes, sizeof(float4) * pl.size(), cudaMemcpyDeviceToHost),
                 "plane read");
     for (size_t e = 0; e < m->nExt && !rc; ++e) {
       const float4 a = pl[2 * e], b = pl[2 * e + 1];
@@ -460,175 +686,290 @@ int vfr_find_visible(vfr_ctx* c, int id, uint32_t* num_vis, uint32_t* visExt, fl
       o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y;
     }
   }
-  if (!rc) C.view.stage = 1;
+  if (!rc) C.stage = 1;
   return rc;
 }
 
 int vfr_project(vfr_ctx* c, int id, uint32_t W, uint32_t H, uint32_t* bbox, int32_t* writer) {
   CTX_OR_FAIL(c);
   Mesh* m = C.mesh(id);
-  if (!m || C.view.mesh != m || C.view.stage < 1)
+  if (!m || C.stage < 1 || !C.plain.njobs || C.plain.specs[0].mesh != id)
     return C.fail(VFR_ERR_STATE, "vfr_project needs vfr_find_visible of the same mesh first");
-  if (W < 2 || H < 2 || (uint64_t)W * H > (1ull << 31))
+  if (W < 2 || H < 2 || (uint64_t)W * H > (1ull << 28))
     return C.fail(VFR_ERR_INVALID, "image size out of range");
-  int rc = C.enqueue_project(C.view, W, H, VFR_MODE_REF);
-  vfr::ViewCounters k;
-  if (!rc) rc = C.read_counters(C.view, k);
+  // the planes and visible list of stage (a) stay where they are: same mesh,
+  // so the same arena offsets; only the pixel arenas grow
+  int rc = single(C, id, nullptr, W, H, VFR_MODE_REF, true, nullptr, nullptr, nullptr);
+  if (!rc) rc = C.plain.enqueue_b();
+  std::vector<vfr::ViewCounters> k;
+  if (!rc) rc = C.plain.counters(k);
   if (rc) return rc;
-  if (bbox && k.nvis)
-    rc = C.cuda(cudaMemcpy(bbox, C.view.bbox.p, sizeof(uint4) * k.nvis, cudaMemcpyDeviceToHost),
+  const vfr::JobDev& J = C.plain.jobs[0];
+  if (bbox && k[0].nvis)
+    rc = C.cuda(cudaMemcpy(bbox, J.bbox, sizeof(uint4) * k[0].nvis, cudaMemcpyDeviceToHost),
                 "bbox read");
   if (!rc && writer)
-    rc = C.cuda(cudaMemcpy(writer, C.view.winner.p, sizeof(int32_t) * (size_t)W * H,
-                           cudaMemcpyDeviceToHost),
+    rc = C.cuda(cudaMemcpy(writer, J.winner, sizeof(int32_t) * (size_t)W * H, cudaMemcpyDeviceToHost),
                 "winner read");
-  if (!rc) C.view.stage = 2;
+  if (!rc) C.stage = 2;
   return rc;
-}
-
-static int copy_outputs(Ctx& C, uint8_t* rgb8, float* rgba, uint32_t* steps, size_t np) {
-  int rc = VFR_OK;
-  if (rgb8)
-    rc = C.cuda(cudaMemcpyAsync(rgb8, C.out_rgb8.p, np * 3, cudaMemcpyDeviceToHost, C.stream),
-                "rgb8 read");
-  if (!rc && rgba)
-    rc = C.cuda(cudaMemcpyAsync(rgba, C.out_rgba.p, np * sizeof(float4), cudaMemcpyDeviceToHost,
-                                C.stream),
-                "rgba read");
-  if (!rc && steps)
-    rc = C.cuda(cudaMemcpyAsync(steps, C.out_steps.p, np * sizeof(uint32_t),
-                                cudaMemcpyDeviceToHost, C.stream),
-                "steps read");
-  if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "output read");
-  return rc;
-}
-
-static int ensure_outputs(Ctx& C, size_t np, bool rgb8, bool rgba, bool steps) {
-  int rc = VFR_OK;
-  if (rgb8) rc = C.grow(C.out_rgb8, np * 3, "rgb8 output");
-  if (!rc && rgba) rc = C.grow(C.out_rgba, np * sizeof(float4), "rgba output");
-  if (!rc && steps) rc = C.grow(C.out_steps, np * sizeof(uint32_t), "steps output");
-  return rc;
-}
-
-static void fill_stats(const vfr::ViewCounters& k, const Mesh& m, vfr_render_stats* s) {
-  s->num_ext = m.nExt;
-  s->num_vis = k.nvis;
-  s->num_rays = k.nrays;
-  s->num_entries = k.nentries;
-  s->num_steps = k.steps;
-  s->device_status = k.status;
 }
 
 int vfr_traverse(vfr_ctx* c, int id, uint8_t* rgb8, float* rgba, uint32_t* steps,
                  vfr_render_stats* stats) {
   CTX_OR_FAIL(c);
   Mesh* m = C.mesh(id);
-  if (!m || C.view.mesh != m || C.view.stage < 2)
+  if (!m || C.stage < 2 || !C.plain.njobs || C.plain.specs[0].mesh != id)
     return C.fail(VFR_ERR_STATE, "vfr_traverse needs vfr_project of the same mesh first");
   if (!C.d_tf) return C.fail(VFR_ERR_STATE, "tables not uploaded");
-  const size_t np = (size_t)C.view.W * C.view.H;
-  int rc = ensure_outputs(C, np, rgb8 != nullptr, rgba != nullptr, steps != nullptr);
-  if (rc) return rc;
+  const size_t np = (size_t)C.plain.specs[0].W * C.plain.specs[0].H;
   cudaEventRecord(C.ev[0], C.stream);
-  rc = C.enqueue_traverse(C.view, rgb8 ? (uint8_t*)C.out_rgb8.p : nullptr,
-                          rgba ? (float4*)C.out_rgba.p : nullptr,
-                          steps ? (uint32_t*)C.out_steps.p : nullptr);
+  int rc = C.plain.enqueue_c();
   cudaEventRecord(C.ev[1], C.stream);
-  vfr::ViewCounters k;
-  if (!rc) rc = C.read_counters(C.view, k);
-  if (!rc) rc = copy_outputs(C, rgb8, rgba, steps, np);
+  std::vector<vfr::ViewCounters> k;
+  if (!rc) rc = C.plain.counters(k);
+  if (!rc) rc = copy_out(C, rgb8, rgba, steps, np);
   if (rc) return rc;
   if (stats) {
     std::memset(stats, 0, sizeof *stats);
-    fill_stats(k, *m, stats);
+    fill_stats(k[0], m->nExt, stats);
     cudaEventElapsedTime(&stats->ms_traverse, C.ev[0], C.ev[1]);
     stats->ms_total = stats->ms_traverse;
   }
-  C.view.stage = 1;  // the ray queue is consumed; project again before another traverse
-  return C.check_status(k);
+  C.stage = 1;  // the ray queue is consumed; project again before another traverse
+  return C.check_status(k[0].status, 0);
 }
 
-static int render_common(Ctx& C, int id, const float* mv16, uint32_t W, uint32_t H, int mode,
-                         uint8_t* rgb8, float4* rgba, uint32_t* steps, int32_t* writer_dev,
-                         bool timed) {
-  Mesh* m = C.mesh(id);
-  if (!m) return C.fail(VFR_ERR_STATE, "unknown mesh id");
+static int render_one(Ctx& C, int id, const float* mv16, uint32_t W, uint32_t H, int mode, bool own,
+                      uint8_t* rgb8, float4* rgba, uint32_t* steps, bool timed) {
+  if (!C.mesh(id)) return C.fail(VFR_ERR_STATE, "unknown mesh id");
   if (!C.d_tf) return C.fail(VFR_ERR_STATE, "tables not uploaded");
-  if (W < 2 || H < 2 || (uint64_t)W * H > (1ull << 31))
-    return C.fail(VFR_ERR_INVALID, "image size out of range");
   if (mode != VFR_MODE_REF && mode != VFR_MODE_COMPOSITED)
     return C.fail(VFR_ERR_INVALID, "unknown mode");
-  if (mode == VFR_MODE_COMPOSITED) {
-    size_t want = C.ent_cap_hint ? C.ent_cap_hint : (size_t)W * H * 4;
-    C.view.ent_cap = want;
-  }
+  C.stage = 0;
+  int rc = single(C, id, mv16, W, H, mode, own, rgb8, rgba, steps);
+  if (rc) return rc;
   if (timed) cudaEventRecord(C.ev[0], C.stream);
   C.prof_mark(0);
-  int rc = C.enqueue_visible(*m, mv16, C.view);
+  rc = C.plain.enqueue_a();
   if (timed) cudaEventRecord(C.ev[1], C.stream);
   C.prof_mark(1);
-  if (!rc) rc = C.enqueue_project(C.view, W, H, mode);
+  if (!rc) rc = C.plain.enqueue_b();
   if (timed) cudaEventRecord(C.ev[2], C.stream);
   C.prof_mark(2);
-  if (!rc) rc = C.enqueue_traverse(C.view, rgb8, rgba, steps);
+  if (!rc) rc = C.plain.enqueue_c();
   if (timed) cudaEventRecord(C.ev[3], C.stream);
   C.prof_mark(3);
-  if (!rc && writer_dev && mode == VFR_MODE_REF)
-    rc = C.cuda(cudaMemcpyAsync(writer_dev, C.view.winner.p, sizeof(int32_t) * (size_t)W * H,
-                                cudaMemcpyDeviceToDevice, C.stream),
-                "winner copy");
-  C.view.stage = 0;
   return rc;
 }
 
 int vfr_render(vfr_ctx* c, int id, const float* mv16, uint32_t W, uint32_t H, int mode,
                uint8_t* rgb8, float* rgba, uint32_t* steps, vfr_render_stats* stats) {
   CTX_OR_FAIL(c);
-  const size_t np = (size_t)W * H;
-  int rc = ensure_outputs(C, np, rgb8 != nullptr, rgba != nullptr, steps != nullptr);
-  if (rc) return rc;
-  rc = render_common(C, id, mv16, W, H, mode, rgb8 ? (uint8_t*)C.out_rgb8.p : nullptr,
-                     rgba ? (float4*)C.out_rgba.p : nullptr,
-                     steps ? (uint32_t*)C.out_steps.p : nullptr, nullptr, true);
-  vfr::ViewCounters k;
-  if (!rc) rc = C.read_counters(C.view, k);
-  if (!rc) rc = copy_outputs(C, rgb8, rgba, steps, np);
-  if (rc) return rc;
-  if (stats) {
-    std::memset(stats, 0, sizeof *stats);
-    fill_stats(k, *C.mesh(id), stats);
-    cudaEventElapsedTime(&stats->ms_visible, C.ev[0], C.ev[1]);
-    cudaEventElapsedTime(&stats->ms_project, C.ev[1], C.ev[2]);
-    cudaEventElapsedTime(&stats->ms_traverse, C.ev[2], C.ev[3]);
-    cudaEventElapsedTime(&stats->ms_total, C.ev[0], C.ev[3]);
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    int rc = render_one(C, id, mv16, W, H, mode, true, nullptr, nullptr, nullptr, true);
+    std::vector<vfr::ViewCounters> k;
+    if (!rc) rc = C.plain.counters(k);
+    if (rc) return rc;
+    if (mode == VFR_MODE_COMPOSITED && k[0].nentries > C.plain.ent_cap) {
+      // entry lists overflowed: grow to the need and render again
+      C.plain.ent_cap = 0;
+      C.ent_cap_hint = k[0].nentries + k[0].nentries / 8 + 1024;
+      continue;
+    }
+    rc = copy_out(C, rgb8, rgba, steps, (size_t)W * H);
+    if (rc) return rc;
+    if (stats) {
+      std::memset(stats, 0, sizeof *stats);
+      fill_stats(k[0], C.mesh(id)->nExt, stats);
+      cudaEventElapsedTime(&stats->ms_visible, C.ev[0], C.ev[1]);
+      cudaEventElapsedTime(&stats->ms_project, C.ev[1], C.ev[2]);
+      cudaEventElapsedTime(&stats->ms_traverse, C.ev[2], C.ev[3]);
+      cudaEventElapsedTime(&stats->ms_total, C.ev[0], C.ev[3]);
+    }
+    return C.check_status(k[0].status, 0);
   }
-  if (mode == VFR_MODE_COMPOSITED && k.nentries > C.view.ent_cap) {
-    // entry lists overflowed: grow to the exact need and render again
-    C.ent_cap_hint = k.nentries + k.nentries / 8;
-    return vfr_render(c, id, mv16, W, H, mode, rgb8, rgba, steps, stats);
-  }
-  return C.check_status(k);
+  return C.fail(VFR_ERR_DEVICE, "entry lists kept overflowing");
 }
 
 int vfr_render_device(vfr_ctx* c, int id, const float* mv16, uint32_t W, uint32_t H, int mode,
                       uint8_t* rgb8_dev, float* rgba_dev, uint32_t* steps_dev, int32_t* writer_dev) {
   CTX_OR_FAIL(c);
-  return render_common(C, id, mv16, W, H, mode, rgb8_dev, (float4*)rgba_dev, steps_dev, writer_dev,
-                       false);
+  int rc = render_one(C, id, mv16, W, H, mode, false, rgb8_dev, (float4*)rgba_dev, steps_dev, false);
+  if (!rc && writer_dev && mode == VFR_MODE_REF)
+    rc = C.cuda(cudaMemcpyAsync(writer_dev, C.plain.jobs[0].winner, sizeof(int32_t) * (size_t)W * H,
+                                cudaMemcpyDeviceToDevice, C.stream),
+                "winner copy");
+  return rc;
 }
 
 int vfr_device_status(vfr_ctx* c, uint32_t* status) {
   CTX_OR_FAIL(c);
-  vfr::ViewCounters k;
-  int rc = C.read_counters(C.view, k);
-  if (rc) return rc;
-  if (status) *status = k.status;
-  if (C.view.mode == VFR_MODE_COMPOSITED && k.nentries > C.view.ent_cap) {
-    C.ent_cap_hint = k.nentries + k.nentries / 8;
-    return C.fail(VFR_ERR_DEVICE, "entry lists overflowed; render again");
+  if (!C.plain.njobs) {
+    if (status) *status = 0;
+    return VFR_OK;
   }
-  return C.check_status(k);
+  std::vector<vfr::ViewCounters> k;
+  int rc = C.plain.counters(k);
+  if (rc) return rc;
+  if (status) *status = k[0].status;
+  const uint32_t over = (C.plain.mode == VFR_MODE_COMPOSITED && k[0].nentries > C.plain.ent_cap);
+  if (over) {
+    C.plain.ent_cap = 0;
+    C.ent_cap_hint = k[0].nentries + k[0].nentries / 8 + 1024;
+  }
+  return C.check_status(k[0].status, over);
+}
+
+// ---- batches ----
+
+int vfr_batch_create(vfr_ctx* c, vfr_batch** out) {
+  CTX_OR_FAIL(c);
+  if (!out) return C.fail(VFR_ERR_INVALID, "null batch pointer");
+  vfr_batch* b = new vfr_batch;
+  b->owner = c;
+  b->b.ctx = &C;
+  C.batches.push_back(b);
+  *out = b;
+  return VFR_OK;
+}
+
+void vfr_batch_destroy(vfr_batch* b) {
+  if (!b) return;
+  if (b->owner) {
+    Ctx& C = b->owner->impl;
+    cudaSetDevice(C.device);
+    cudaStreamSynchronize(C.stream);
+    C.batches.erase(std::remove(C.batches.begin(), C.batches.end(), (void*)b), C.batches.end());
+  }
+  delete b;
+}
+
+int vfr_batch_set_jobs(vfr_batch* b, const vfr_job* jobs, uint32_t n, int mode) {
+  if (!b) return VFR_ERR_INVALID;
+  if (!b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  if (!jobs || n == 0) return C.fail(VFR_ERR_INVALID, "empty job list");
+  if (mode != VFR_MODE_REF && mode != VFR_MODE_COMPOSITED)
+    return C.fail(VFR_ERR_INVALID, "unknown mode");
+  std::vector<JobSpec> s(n);
+  bool own = false;
+  for (uint32_t j = 0; j < n; ++j) {
+    s[j].mesh = jobs[j].mesh_id;
+    s[j].W = jobs[j].W;
+    s[j].H = jobs[j].H;
+    s[j].use_mv = jobs[j].use_mv != 0;
+    std::memcpy(s[j].mv, jobs[j].mv, sizeof s[j].mv);
+    s[j].rgb8 = jobs[j].rgb8_dev;
+    s[j].rgba = (float4*)jobs[j].rgba_dev;
+    s[j].steps = jobs[j].steps_dev;
+    own = own || (!jobs[j].rgb8_dev && !jobs[j].rgba_dev && !jobs[j].steps_dev);
+  }
+  cudaStreamSynchronize(C.stream);
+  int rc = b->b.layout(s, mode, own);
+  if (!rc) rc = b->b.upload(false);
+  return rc;
+}
+
+int vfr_batch_capture(vfr_batch* b) {
+  if (!b || !b->b.njobs) return VFR_ERR_STATE;
+  if (!b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  if (!C.d_tf) return C.fail(VFR_ERR_STATE, "tables not uploaded");
+  return b->b.capture();
+}
+
+int vfr_batch_run(vfr_batch* b) {
+  if (!b || !b->b.njobs) return VFR_ERR_STATE;
+  if (!b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  if (!C.d_tf) return C.fail(VFR_ERR_STATE, "tables not uploaded");
+  if (C.profile && !b->b.exec) {  // per-stage events need the direct launches
+    C.prof_mark(0);
+    int rc = b->b.enqueue_a();
+    C.prof_mark(1);
+    if (!rc) rc = b->b.enqueue_b();
+    C.prof_mark(2);
+    if (!rc) rc = b->b.enqueue_c();
+    C.prof_mark(3);
+    return rc;
+  }
+  C.prof_mark(0);
+  C.prof_mark(1);
+  C.prof_mark(2);
+  int rc = b->b.run();
+  C.prof_mark(3);
+  return rc;
+}
+
+int vfr_batch_stats(vfr_batch* b, vfr_render_stats* per_job, uint32_t n) {
+  if (!b || !b->b.njobs) return VFR_ERR_STATE;
+  if (!b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  std::vector<vfr::ViewCounters> k;
+  int rc = b->b.counters(k);
+  if (rc) return rc;
+  uint32_t status = 0, over = 0;
+  for (uint32_t j = 0; j < b->b.njobs; ++j) {
+    status |= k[j].status;
+    if (j < n && per_job) {
+      std::memset(&per_job[j], 0, sizeof per_job[j]);
+      fill_stats(k[j], b->b.jobs[j].nExt, &per_job[j]);
+    }
+  }
+  if (b->b.mode == VFR_MODE_COMPOSITED) {
+    uint64_t tot = 0;
+    for (auto& x : k) tot += x.nentries;
+    over = tot > b->b.ent_cap;
+  }
+  return C.check_status(status, over);
+}
+
+int vfr_batch_output(vfr_batch* b, uint32_t job, uint8_t** rgb8_dev, float** rgba_dev,
+                     uint32_t** steps_dev) {
+  if (!b || job >= b->b.njobs) return VFR_ERR_STATE;
+  if (rgb8_dev) *rgb8_dev = b->b.specs[job].rgb8;
+  if (rgba_dev) *rgba_dev = (float*)b->b.specs[job].rgba;
+  if (steps_dev) *steps_dev = b->b.specs[job].steps;
+  return VFR_OK;
+}
+
+int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host, uint32_t* steps_host) {
+  if (!b || !b->b.njobs) return VFR_ERR_STATE;
+  if (!b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  size_t off = 0;
+  int rc = VFR_OK;
+  for (uint32_t j = 0; j < b->b.njobs && !rc; ++j) {
+    const JobSpec& q = b->b.specs[j];
+    const size_t np = (size_t)q.W * q.H;
+    if (rgb8_host && q.rgb8)
+      rc = C.cuda(cudaMemcpyAsync(rgb8_host + 3 * off, q.rgb8, 3 * np, cudaMemcpyDeviceToHost,
+                                  C.stream),
+                  "rgb8 read");
+    if (!rc && rgba_host && q.rgba)
+      rc = C.cuda(cudaMemcpyAsync(rgba_host + 4 * off, q.rgba, sizeof(float4) * np,
+                                  cudaMemcpyDeviceToHost, C.stream),
+                  "rgba read");
+    if (!rc && steps_host && q.steps)
+      rc = C.cuda(cudaMemcpyAsync(steps_host + off, q.steps, sizeof(uint32_t) * np,
+                                  cudaMemcpyDeviceToHost, C.stream),
+                  "steps read");
+    off += np;
+  }
+  if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "batch read");
+  return rc;
+}
+
+int vfr_batch_scratch_bytes(vfr_batch* b, uint64_t* bytes) {
+  if (!b || !bytes) return VFR_ERR_INVALID;
+  *bytes = b->b.scratch_bytes;
+  return VFR_OK;
 }
 
 }  // extern "C"

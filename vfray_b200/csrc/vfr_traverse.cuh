@@ -12,9 +12,23 @@
 // the next tet does not share with this one (its id is in this tet's record),
 // so one memory round trip per step.
 #pragma once
-#include "vfr_device.cuh"
+#include "vfr_jobs.cuh"
 
 namespace vfr {
+
+struct TraverseParams {
+  const JobDev* jobs;
+  uint32_t njobs;
+  const uint32_t* ray_pref;  // njobs + 1, exclusive prefix of the jobs' ray counts
+  uint32_t* queue;           // work-queue head over all jobs' rays
+  const uint2* ent;          // composited: entry arena (z bits, ext face)
+  uint32_t ent_cap;
+  const float4* tf;          // 256 RGBA
+  const float* psi;          // 512 x 512
+  uint32_t psi_one;          // psi[0][0] == 1 (zero-extinction shortcut allowed)
+  uint32_t step_cap;         // 0: 4 * nT + 64 of each job's mesh
+  uint32_t refill;           // refill a warp's idle lanes once this many are idle
+};
 
 // One exit candidate (vfRayKernelCPU.cc:312-348), branch-free.  The slack
 // test (double)(c1+c2) <= (double)cr + 1e-12 is decided in float unless cr is
@@ -52,6 +66,10 @@ __device__ __forceinline__ uint32_t pick3u(uint32_t i, uint32_t x1, uint32_t x2,
 struct Ray {
   float4 r0, r1, r2, r3;       // vertices rotated by the entry face
   WalkRec w;                   // walk record of the current tet
+  const WalkRec* walk;         // this job's mesh and view vertices
+  const float4* vert;
+  uint32_t j, nT, cap;
+  float maxEdge;
   float4 cb;                   // colorBack
   uint32_t t, f, p, iters;
   float ox, oy, zp, sp;
@@ -62,17 +80,17 @@ struct Ray {
 };
 
 // Start a segment at external face e with entry depth zp (:256-279).
-__device__ __forceinline__ void begin_segment(const TraverseParams& P, const float4* s_tf, Ray& R,
+__device__ __forceinline__ void begin_segment(const JobDev& J, const float4* s_tf, Ray& R,
                                               uint32_t e, float zp, float sp) {
-  const uint2 tf = P.extf[e];
+  const uint2 tf = J.extf[e];
   R.t = tf.x;
   R.f = tf.y;
-  const uint4 id = P.tet[R.t];
-  R.w = P.walk[R.t];
-  R.r0 = P.vert[sel4(id, R.f)];
-  R.r1 = P.vert[sel4(id, (R.f + 1) & 3u)];
-  R.r2 = P.vert[sel4(id, (R.f + 2) & 3u)];
-  R.r3 = P.vert[sel4(id, (R.f + 3) & 3u)];
+  const uint4 id = J.tet[R.t];
+  R.w = R.walk[R.t];
+  R.r0 = R.vert[sel4(id, R.f)];
+  R.r1 = R.vert[sel4(id, (R.f + 1) & 3u)];
+  R.r2 = R.vert[sel4(id, (R.f + 2) & 3u)];
+  R.r3 = R.vert[sel4(id, (R.f + 3) & 3u)];
   R.zp = zp;
   R.sp = sp;
   R.lastZ = zp;
@@ -82,8 +100,8 @@ __device__ __forceinline__ void begin_segment(const TraverseParams& P, const flo
 // Composited mode: the next entry of the pixel in (depth, index) descending
 // order after the last one taken, skipping entries above the depth where the
 // previous segment left the mesh.  Returns false when the list is done.
-__device__ __forceinline__ bool next_entry(const TraverseParams& P, const float4* s_tf, Ray& R,
-                                           bool first) {
+__device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev& J,
+                                           const float4* s_tf, Ray& R, bool first) {
   for (;;) {
     float bz = -INFINITY;
     uint32_t be = 0, bzb = 0;
@@ -106,31 +124,31 @@ __device__ __forceinline__ bool next_entry(const TraverseParams& P, const float4
     R.de = be;
     first = false;
     if (bz > R.exitZ) continue;  // behind the ray already
-    const float4 p0 = P.planes[2 * (size_t)be], p1 = P.planes[2 * (size_t)be + 1];
-    begin_segment(P, s_tf, R, be, bz, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
+    const float4 p0 = J.planes[2 * (size_t)be], p1 = J.planes[2 * (size_t)be + 1];
+    begin_segment(J, s_tf, R, be, bz, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
     return true;
   }
 }
 
-__device__ __forceinline__ void finish_pixel(const TraverseParams& P, const Ray& R) {
+__device__ __forceinline__ void finish_pixel(const JobDev& J, const Ray& R) {
   float c[3] = {R.ar, R.ag, R.ab};
 #pragma unroll
   for (int k = 0; k < 3; ++k) c[k] = (c[k] > 1.0f) ? 1.0f : c[k];  // :546-548
-  if (P.rgb8) {
-    uint8_t* o = P.rgb8 + 3 * (size_t)R.p;
+  if (J.rgb8) {
+    uint8_t* o = J.rgb8 + 3 * (size_t)R.p;
 #pragma unroll
     for (int k = 0; k < 3; ++k) o[k] = (uint8_t)__float2int_rz(fmul(255.0f, c[k]));  // :550-552
   }
-  if (P.rgba) P.rgba[R.p] = make_float4(c[0], c[1], c[2], fsub(1.0f, R.tr));
-  if (P.steps) P.steps[R.p] = R.iters;
+  if (J.rgba) J.rgba[R.p] = make_float4(c[0], c[1], c[2], fsub(1.0f, R.tr));
+  if (J.steps) J.steps[R.p] = R.iters;
 }
 
 enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kAbandon = 2, kCap = 3, kRange = 4 };
 
 // One iteration of the reference's while loop (:302-542).
-__device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* s_tf, float maxEdge,
-                                         bool psi_one, Ray& R) {
-  if (++R.iters > P.step_cap) return kCap;
+__device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* s_tf, bool psi_one,
+                                         Ray& R) {
+  if (++R.iters > R.cap) return kCap;
   const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
   const bool h3 = exit_test(R.r3, R.r0, R.r1, R.ox, R.oy);
@@ -140,13 +158,13 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* 
   const uint32_t tn = sel4(R.w.n, ex);
   const uint32_t q = sel4(R.w.q, ex);
   const bool leaving = (tn == R.t);
-  if (tn >= P.nT) return kRange;
+  if (tn >= R.nT) return kRange;
   // both loads of the step, issued before the plane solve that hides them
   WalkRec N = R.w;
   float4 nv = R.r0;
   if (!leaving) {
-    N = P.walk[tn];
-    nv = P.vert[q & 0x07ffffffu];
+    N = R.walk[tn];
+    nv = R.vert[q & 0x07ffffffu];
   }
   // exit face (ex, ex+1, ex+2) = (r_i, r_i+1, r_i+2)
   const float4 a = pick3(i, R.r1, R.r2, R.r3);
@@ -160,7 +178,7 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* 
   dz = dz < 0.0f ? -dz : dz;
   dz = below_rdelta(dz) ? 0.0f : dz;
   if ((sn < 0.0f) || (sn > 1.0f)) return kSegmentEnd;  // :446
-  dz = (dz == 0.0f) ? 0.0f : fdiv(dz, maxEdge);
+  dz = (dz == 0.0f) ? 0.0f : fdiv(dz, R.maxEdge);
   const float4 cf = s_tf[(uint32_t)fmul(255.0f, sn)];
   const float taux = fmul(cf.w, dz), tauy = fmul(R.cb.w, dz);
   if (!(psi_one && taux == 0.0f && tauy == 0.0f)) {
@@ -207,11 +225,11 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* 
     R.r2 = m2 == 0 ? a : (m2 == 1 ? b : c);
     R.r3 = nv;
   } else {  // shared face not matched by vertex ids: reload the tet's vertices
-    const uint4 id = P.tet[tn];
-    R.r0 = P.vert[sel4(id, fn)];
-    R.r1 = P.vert[sel4(id, (fn + 1) & 3u)];
-    R.r2 = P.vert[sel4(id, (fn + 2) & 3u)];
-    R.r3 = P.vert[sel4(id, (fn + 3) & 3u)];
+    const uint4 id = P.jobs[R.j].tet[tn];
+    R.r0 = R.vert[sel4(id, fn)];
+    R.r1 = R.vert[sel4(id, (fn + 1) & 3u)];
+    R.r2 = R.vert[sel4(id, (fn + 2) & 3u)];
+    R.r3 = R.vert[sel4(id, (fn + 3) & 3u)];
   }
   R.w = N;
   R.t = tn;
@@ -221,8 +239,26 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* 
   return kContinue;
 }
 
+// Per-lane tallies of tet-walk steps and status bits, flushed to the job's
+// counters when the lane moves to another job and at the end.
+struct Tally {
+  uint32_t j;
+  unsigned long long steps;
+  uint32_t status;
+};
+
+__device__ __forceinline__ void flush(const TraverseParams& P, Tally& T) {
+  if (T.j != 0xffffffffu) {
+    ViewCounters* c = P.jobs[T.j].ctr;
+    if (T.steps) atomicAdd(&c->steps, T.steps);
+    if (T.status) atomicOr(&c->status, T.status);
+  }
+  T.steps = 0;
+  T.status = 0;
+}
+
 // kMinBlocks: CTAs of 256 threads the register budget must allow per SM
-// (2: ~104 registers, no spills; 3: 80 registers, a few spilled to L1).
+// (2: no spills; 3: 80 registers, a few spilled to L1).
 template <int kMode, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParams P) {
   __shared__ float4 s_tf[256];
@@ -230,12 +266,10 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt_mask = (1u << lane) - 1u;
-  const uint32_t nrays = P.ctr->nrays;
-  const float maxEdge = P.use_view_maxedge ? __uint_as_float(P.ctr->maxedge_bits) : P.maxEdge;
+  const uint32_t nrays = P.ray_pref[P.njobs];
   const uint32_t refill = P.refill ? P.refill : 1u;
   const bool psi_one = P.psi_one != 0;
-  unsigned long long my_steps = 0;
-  uint32_t status = 0;
+  Tally T = {0xffffffffu, 0ull, 0u};
   bool active = false, exhausted = false;
   Ray R;
   for (;;) {
@@ -243,37 +277,49 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
     if (idle && !exhausted && ((uint32_t)__popc(idle) >= refill || idle == 0xffffffffu)) {
       const uint32_t leader = __ffs(idle) - 1u, k = __popc(idle);
       uint32_t base = 0;
-      if (lane == leader) base = atomicAdd(&P.ctr->queue, k);
+      if (lane == leader) base = atomicAdd(P.queue, k);
       base = __shfl_sync(0xffffffffu, base, leader);
       if (base + k >= nrays) exhausted = true;
       if (!active) {
-        const uint32_t rr = base + __popc(idle & lt_mask);
-        if (rr < nrays) {
-          R.p = P.rays[rr];
-          const uint32_t x = R.p % P.W, y = R.p / P.W;
-          R.ox = obj_coord(x, P.W);
-          R.oy = obj_coord(y, P.H);
+        const uint32_t g = base + __popc(idle & lt_mask);
+        if (g < nrays) {
+          const uint32_t j = job_of(P.ray_pref, P.njobs, g);
+          const JobDev& J = P.jobs[j];
+          if (j != T.j) {
+            flush(P, T);
+            T.j = j;
+          }
+          R.j = j;
+          R.walk = J.walk;
+          R.vert = J.vert;
+          R.nT = J.nT;
+          R.cap = P.step_cap ? P.step_cap : min(4u * J.nT + 64u, 0x7fffffffu);
+          R.maxEdge = job_maxedge(J);
+          R.p = J.rays[g - P.ray_pref[j]];
+          const uint32_t x = R.p % J.W, y = R.p / J.W;
+          R.ox = obj_coord(x, J.W);
+          R.oy = obj_coord(y, J.H);
           R.ar = R.ag = R.ab = 0.0f;
           R.tr = 1.0f;
           R.iters = 0;
           if (kMode == 0) {
-            const uint32_t e = (uint32_t)P.winner[R.p];
-            const float4 p0 = P.planes[2 * (size_t)e], p1 = P.planes[2 * (size_t)e + 1];
-            begin_segment(P, s_tf, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
+            const uint32_t e = (uint32_t)J.winner[R.p];
+            const float4 p0 = J.planes[2 * (size_t)e], p1 = J.planes[2 * (size_t)e + 1];
+            begin_segment(J, s_tf, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
                           plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
             active = true;
           } else {
-            R.ea = P.ent_off[R.p];
-            const uint32_t b1 = P.ent_off[R.p + 1];
+            R.ea = J.ent_off[R.p];
+            const uint32_t b1 = J.ent_off[R.p + 1];
             R.en = b1 - R.ea;
             R.exitZ = INFINITY;
             R.dz_bits = 0;
             R.de = 0;
             if (b1 > P.ent_cap) {
-              status |= 16u;  // VFR_DEV_OVERFLOW: the caller renders again with room
+              T.status |= 16u;  // VFR_DEV_OVERFLOW: the caller renders again with room
             } else {
-              active = next_entry(P, s_tf, R, true);
-              if (!active) finish_pixel(P, R);
+              active = next_entry(P, J, s_tf, R, true);
+              if (!active) finish_pixel(J, R);
             }
           }
         }
@@ -284,28 +330,26 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
       continue;
     }
     if (!active) continue;
-    const uint32_t res = step(P, s_tf, maxEdge, psi_one, R);
+    const uint32_t res = step(P, s_tf, psi_one, R);
     if (res == kContinue) continue;
     if (res == kSegmentEnd) {
       if (kMode == 1) {
         R.exitZ = R.lastZ;
-        if (next_entry(P, s_tf, R, false)) continue;
+        if (next_entry(P, P.jobs[R.j], s_tf, R, false)) continue;
       }
-      finish_pixel(P, R);
+      finish_pixel(P.jobs[R.j], R);
     } else if (res == kAbandon) {
-      status |= 1u;  // the reference writes nothing for this pixel (:365)
+      T.status |= 1u;  // the reference writes nothing for this pixel (:365)
     } else if (res == kCap) {
-      status |= 2u;
-      finish_pixel(P, R);
+      T.status |= 2u;
+      finish_pixel(P.jobs[R.j], R);
     } else {
-      status |= 4u;
+      T.status |= 4u;
     }
-    my_steps += R.iters;
+    T.steps += R.iters;
     active = false;
   }
-  for (int o = 16; o; o >>= 1) my_steps += __shfl_xor_sync(0xffffffffu, my_steps, o);
-  if (lane == 0 && my_steps) atomicAdd(&P.ctr->steps, my_steps);
-  if (status) atomicOr(&P.ctr->status, status);
+  flush(P, T);
 }
 
 }  // namespace vfr
