@@ -1,12 +1,19 @@
 """Benchmark of the VF-Ray render path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--form batched|plain] [--workload orbit64|convex24]
+                    [--form batched|plain] [--workload orbit64|mixed|served|convex24]
 
-Workload (default ``orbit64``): the carved 64^3 Freudenthal mesh (1,572,864
-tets before carving at the 85th percentile of a 16-Gaussian field) seen from
-64 seeded orbit views at 512x512, fp32 colour + RGB8.  One step renders all
-64 views.  ``convex24`` is the single 512x512 view of the convex 24^3 mesh.
+Workloads (seeded synthetic meshes, transfer function and cameras):
+  orbit64  (default) the carved 64^3 Freudenthal mesh (1,572,864 tets before
+           carving at the 85th percentile of a 16-Gaussian field) seen from 64
+           seeded orbit views at 512x512; one step renders the 64 views.
+  mixed    8 carved meshes with 16..128 cells per side and 256 jobs, each a
+           random mesh, resolution in {128^2, 256^2, 512^2, 1024^2} and
+           rotation; one step renders the 256 jobs.
+  served   the mixed meshes behind the request loop: Poisson arrivals at
+           several rates, requests at {256^2, 512^2, 1024^2}; p50/p99 latency
+           and Mrays/s per rate.
+  convex24 one 512x512 view of the convex 24^3 mesh.
 
 Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events
 on the render stream after an L2 flush (a 256 MiB write) that is not timed;
@@ -14,12 +21,12 @@ the step times are summed, the max over ranks is taken (N > 1 runs N
 replicas, one per GPU, weak scaling), and ``value`` = rays rendered by all
 ranks / that time.  A ray is a pixel with an entry face.  ``e2e`` is the same
 metric through the host-buffer API (camera in, RGB8 images out through pinned
-host memory, copies inside the timed region).  ``roofline`` divides the
-traversal kernel's algorithmic bytes (48 B per tet-walk step: one 32-byte tet
-record + one new 16-byte vertex) by its event-timed launch durations.
+host memory, the copies inside the timed region).  ``roofline`` divides the
+traversal kernel's algorithmic bytes (48 B per tet-walk step: one 32-byte walk
+record + one new 16-byte vertex) by its event-timed launch duration.
 ``cpu_baseline`` times the reference's own CPU kernels (built from the
 reference sources into oracle/_ref, -O3 -ffast-math as the reference builds
-them) on all host cores over a bounded sample of the same views.
+them) on all host cores over a bounded sample of the same jobs.
 """
 from __future__ import annotations
 
@@ -35,7 +42,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_STEP = 48        # 32-byte tet record + one new 16-byte vertex
+BYTES_PER_STEP = 48        # 32-byte walk record + one new 16-byte vertex
 FLUSH_BYTES = 256 << 20    # > 126 MB L2
 
 
@@ -46,33 +53,68 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
-    ap.add_argument("--workload", default="orbit64", choices=["orbit64", "convex24"])
+    ap.add_argument("--workload", default="orbit64",
+                    choices=["orbit64", "mixed", "served", "convex24"])
+    ap.add_argument("--views", type=int, default=64, help="orbit views (orbit64)")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="bound of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rates", default="50,200,1000,2000", help="served: arrival rates (req/s)")
+    ap.add_argument("--served-seconds", type=float, default=2.0)
     return ap.parse_args()
 
 
-# ------------------------------------------------------------------ workload
+# ------------------------------------------------------------------ workloads
 
-def make_workload(name):
+MIXED_N = (16, 24, 32, 48, 64, 80, 96, 128)
+
+
+def _mesh(n, carved, seed_offset=0):
     import vfray_b200 as vb
     from vfray_b200 import synth
 
-    if name == "orbit64":
-        vert, tet = synth.make_mesh(64, carved=True, view_seed=None)
-        views = synth.orbit_views(64, seed=3)
-        W = H = 512
-        desc = "64 orbit views at 512x512 of the carved 64^3 Freudenthal mesh"
-    else:
-        vert, tet = synth.make_mesh(24, carved=False, view_seed=3)
-        views = [None]
-        W = H = 512
-        desc = "one 512x512 view of the convex 24^3 Freudenthal mesh (seeded rotation)"
+    vert, tet = synth.make_mesh(n, carved=carved, view_seed=None, jitter_seed=0 + seed_offset,
+                                scalar_seed=1 + seed_offset, carve_seed=4 + seed_offset)
     p = vb.prepare(vert, tet)
-    p.update(tf=synth.transfer_function(2), psi=vb.psi_table(), views=views, W=W, H=H,
-             name=name, desc=desc)
+    p["n"] = n
     return p
+
+
+def make_workload(name, views=64):
+    """Meshes (prepared as vfRayPreComp would) and jobs (mesh index, model-view
+    or None, W, H)."""
+    import vfray_b200 as vb
+    from vfray_b200 import synth
+
+    wl = dict(name=name, tf=synth.transfer_function(2), psi=vb.psi_table())
+    if name == "orbit64":
+        wl["meshes"] = [_mesh(64, True)]
+        wl["jobs"] = [(0, mv, 512, 512) for mv in synth.orbit_views(views, seed=3)]
+        wl["desc"] = f"{views} orbit views at 512x512 of the carved 64^3 Freudenthal mesh"
+    elif name == "convex24":
+        vert, tet = synth.make_mesh(24, carved=False, view_seed=3)
+        p = vb.prepare(vert, tet)
+        p["n"] = 24
+        wl["meshes"] = [p]
+        wl["jobs"] = [(0, None, 512, 512)]
+        wl["desc"] = "one 512x512 view of the convex 24^3 Freudenthal mesh (seeded rotation)"
+    else:  # mixed / served
+        wl["meshes"] = [_mesh(n, True, seed_offset=k) for k, n in enumerate(MIXED_N)]
+        rng = np.random.default_rng(5)
+        res = (128, 256, 512, 1024)
+        jobs = []
+        for j in range(256):
+            m = int(rng.integers(len(MIXED_N)))
+            r = int(res[rng.integers(len(res))])
+            q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+            mv = np.eye(4, dtype=np.float32)
+            mv[:3, :3] = q * np.sign(np.linalg.det(q))
+            jobs.append((m, mv, r, r))
+        wl["jobs"] = jobs
+        wl["desc"] = ("256 jobs over 8 carved meshes (16..128 cells per side), resolutions "
+                      "128^2..1024^2, random rotations")
+    return wl
 
 
 def load_peaks():
@@ -84,13 +126,13 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic():
+def load_traffic(name):
     """Per-launch DRAM bytes of the traversal kernel from the committed ncu
-    summary, scaled per step of the workload, if present."""
+    summary of this workload, if present."""
     path = os.path.join(ROOT, "profiles", "traverse_traffic.json")
     if os.path.exists(path):
         with open(path) as f:
-            return json.load(f)
+            return json.load(f).get(name)
     return None
 
 
@@ -149,53 +191,61 @@ class Clocks:
 
 # ------------------------------------------------------------------ ours
 
-def run_ours(args, rank, world, dist):
+def setup_gpu(wl, dev):
     import torch
 
     import vfray_b200 as vb
 
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    wl = make_workload(args.workload)
-    W, H, views = wl["W"], wl["H"], wl["views"]
     stream = torch.cuda.Stream(device=dev)
-    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-
     r = vb.Renderer(dev)
     r.set_stream(stream)
     r.upload_tables(wl["tf"], wl["psi"])
-    mid = r.upload_mesh(wl["vert"], wl["tet"], wl["con"], wl["extf"], wl["lmt"])
-    nv = len(views)
+    mids = [r.upload_mesh(p["vert"], p["tet"], p["con"], p["extf"], p["lmt"]) for p in wl["meshes"]]
+    return r, stream, mids
 
-    # reference counts per view (rays, steps) from one checked pass
-    rays_v, steps_v = [], []
-    for mv in views:
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    import vfray_b200 as vb
+    from vfray_b200 import batch as vbatch
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = make_workload(args.workload, args.views)
+    r, stream, mids = setup_gpu(wl, dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    jobs = [(mids[m], mv, W, H) for (m, mv, W, H) in wl["jobs"]]
+    nj = len(jobs)
+
+    # per-job rays and steps from single-view renders (checked below against the batch)
+    rays_j, steps_j = [], []
+    for (mid, mv, W, H) in jobs:
         o = r.render(mid, W, H, mv=mv, rgba=False, steps=False)
-        rays_v.append(o["stats"]["num_rays"])
-        steps_v.append(o["stats"]["num_steps"])
-    rays_step, steps_step = int(sum(rays_v)), int(sum(steps_v))
-
-    rgb_d = torch.empty((nv, H, W, 3), dtype=torch.uint8, device=dev)
-    rgba_d = torch.empty((nv, H, W, 4), dtype=torch.float32, device=dev)
-
-    if args.form == "batched":
-        from vfray_b200 import batch as vbatch
-
-        runner = vbatch.BatchRenderer(r, [(mid, mv, W, H) for mv in views])
-        runner.prepare()
-
-        def step_plain_or_batched():
-            runner.run(rgb_d, rgba_d)
-        launches_per_step = runner.launches_per_run()
-    else:
-        def step_plain_or_batched():
-            for i, mv in enumerate(views):
-                r.render_device(mid, W, H, mv=mv, rgb8=rgb_d[i], rgba=rgba_d[i])
-        launches_per_step = 11 * nv
+        rays_j.append(o["stats"]["num_rays"])
+        steps_j.append(o["stats"]["num_steps"])
+    rays_step, steps_step = int(sum(rays_j)), int(sum(steps_j))
+    npix = sum(W * H for (_, _, W, H) in jobs)
+    offs = np.cumsum([0] + [W * H for (_, _, W, H) in jobs])
+    rgb_d = torch.empty(npix * 3, dtype=torch.uint8, device=dev)
+    rgba_d = torch.empty(npix * 4, dtype=torch.float32, device=dev)
 
     def plain_step():
-        for i, mv in enumerate(views):
-            r.render_device(mid, W, H, mv=mv, rgb8=rgb_d[i], rgba=rgba_d[i])
+        for i, (mid, mv, W, H) in enumerate(jobs):
+            r.render_device(mid, W, H, mv=mv, rgb8=rgb_d[3 * offs[i]:3 * offs[i + 1]],
+                            rgba=rgba_d[4 * offs[i]:4 * offs[i + 1]])
+
+    tuning = None
+    runner = vbatch.BatchRenderer(r, jobs)
+    if not args.no_autotune:
+        tuning = runner.autotune(reps=1)
+    runner.prepare()
+
+    def batched_step():
+        runner.run()
+
+    step = batched_step if args.form == "batched" else plain_step
+    launches_per_step = runner.launches_per_run() if args.form == "batched" else 11 * nj
 
     def timed(fn, K, Wu, profile=False):
         for _ in range(Wu):
@@ -225,34 +275,31 @@ def run_ours(args, rank, world, dist):
     if dist:
         dist.barrier()
     with Clocks(dev) as clk:
-        t_main, _ = timed(step_plain_or_batched, args.steps, args.warmup)
-    if args.form == "batched":
-        bst = runner.stats()  # raises on any device status of the batch
-        assert sum(x["num_rays"] for x in bst) == rays_step, "batched rays differ from single views"
-        assert sum(x["num_steps"] for x in bst) == steps_step, "batched steps differ"
-    t_plain, prof_plain = timed(plain_step, max(1, min(args.steps, 3)), 1, profile=True)
-    if args.form == "batched":
-        # stage times of the batched chain: the same batch launched directly
-        # (not as a graph) with events between its stages
-        runner_p = vbatch.BatchRenderer(r, [(mid, mv, W, H) for mv in views], graph=False)
-        _, prof = timed(lambda: runner_p.run(), max(1, min(args.steps, 3)), 1, profile=True)
-        runner_p.close()
-        launches_per_trav = 1
-    else:
-        prof = prof_plain
-        launches_per_trav = nv
+        t_main, _ = timed(step, args.steps, args.warmup)
+    bst = runner.stats()  # raises on any device status of the batch
+    assert sum(x["num_rays"] for x in bst) == rays_step, "batched rays differ from single views"
+    assert sum(x["num_steps"] for x in bst) == steps_step, "batched steps differ"
+    kp = max(1, min(args.steps, 3))
+    t_plain, prof_plain = timed(plain_step, kp, 1, profile=True)
+    t_batch, _ = timed(batched_step, kp, 1)
+    # stage times of the batched chain: the same batch launched directly
+    # (not as a graph) with events between its stages
+    runner_p = vbatch.BatchRenderer(r, jobs, graph=False)
+    _, prof_batch = timed(lambda: runner_p.run(), kp, 1, profile=True)
+    runner_p.close()
+    prof, launches_per_trav = (prof_batch, 1) if args.form == "batched" else (prof_plain, nj)
 
-    # e2e through the host API: camera in, RGB8 out (pinned), copies timed
-    pinned = torch.empty((nv, H, W, 3), dtype=torch.uint8, pin_memory=True)
+    # e2e through the host API: cameras in, RGB8 out through pinned memory
+    pinned = torch.empty(npix * 3, dtype=torch.uint8, pin_memory=True)
     if args.form == "batched":
         def e2e_step():
             runner.run_host(pinned)
     else:
-        host_bufs = [pinned[i].numpy() for i in range(nv)]
+        host = pinned.numpy()
 
         def e2e_step():
-            for i, mv in enumerate(views):
-                r.render_into_host(mid, W, H, host_bufs[i], mv=mv)
+            for i, (mid, mv, W, H) in enumerate(jobs):
+                r.render_into_host(mid, W, H, host[3 * offs[i]:3 * offs[i + 1]], mv=mv)
     for _ in range(max(1, args.warmup)):
         e2e_step()
     t0 = time.perf_counter()
@@ -260,157 +307,210 @@ def run_ours(args, rank, world, dist):
         e2e_step()
     t_e2e = (time.perf_counter() - t0) * 1e3
 
-    times = np.array([t_main, t_e2e, t_plain], dtype=np.float64)
+    times = np.array([t_main, t_e2e, t_plain, t_batch], dtype=np.float64)
     if dist:
         import torch.distributed as td
 
         tt = torch.tensor(times, device=dev)
         td.all_reduce(tt, op=td.ReduceOp.MAX)
         times = tt.cpu().numpy()
-    t_main, t_e2e, t_plain = times
+    t_main, t_e2e, t_plain, t_batch = times
     K = args.steps
-    value = rays_step * world * K / (t_main * 1e-3) / 1e6
-    e2e = rays_step * world * K / (t_e2e * 1e-3) / 1e6
-    plain = rays_step * world * max(1, min(K, 3)) / (t_plain * 1e-3) / 1e6
 
-    # roofline of the traversal kernel: algorithmic bytes of a launch over its
-    # event-timed duration (batched: one launch covers all views)
+    def mrays(t, k):
+        return rays_step * world * k / (t * 1e-3) / 1e6
+
+    value, e2e = mrays(t_main, K), mrays(t_e2e, K)
+
     peak, peak_kind = load_peaks()
     trav_ms = prof[:, 2] if prof is not None and len(prof) else None
     roof = None
     if trav_ms is not None:
         bytes_per_launch = BYTES_PER_STEP * steps_step / launches_per_trav
         achieved = bytes_per_launch * len(trav_ms) / (trav_ms.sum() * 1e-3) / 1e9
-        traffic = load_traffic()
         roof = {"bound": "hbm", "achieved": round(float(achieved), 1), "peak": peak, "unit": "GB/s",
                 "frac": round(float(achieved / peak), 4),
                 "peak_kind": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                               else "fallback 6.65 TB/s"),
-                "traffic": None if traffic is None else traffic.get("bytes_per_launch"),
+                "traffic": load_traffic(wl["name"]),
                 "algorithmic_bytes_per_launch": int(bytes_per_launch),
                 "bytes_per_step": BYTES_PER_STEP,
-                "kernel": "vfr::traverse_kernel<0,2>" + (" (one launch for all views)"
-                                                        if launches_per_trav == 1 else " (per view)"),
+                "kernel": "vfr::traverse_kernel<0,2>" + (" (one launch for all jobs)"
+                                                        if launches_per_trav == 1 else " (per job)"),
                 "launch_ms_mean": round(float(trav_ms.mean()), 4),
                 "gsteps_per_s": round(float(steps_step / launches_per_trav * len(trav_ms)
                                             / (trav_ms.sum() * 1e-3) / 1e9), 2),
                 "stage_ms_mean": [round(float(x), 4) for x in prof.mean(0)]}
-    if args.form == "batched":
-        runner.close()
-    r.release_mesh(mid)
+    runner.close()
+    for m in mids:
+        r.release_mesh(m)
     r.close()
     if rank != 0:
         return None
     out = {
-        "metric": f"Mrays/s ({wl['desc']})", "value": round(value, 2), "unit": "Mrays/s",
+        "metric": f"Mrays/s ({wl['desc']})", "value": round(float(value), 2), "unit": "Mrays/s",
         "n_gpus": world, "steps": K, "warmup": args.warmup,
-        "ms_per_step": round(t_main / K, 3), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": round(float(t_main / K), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded meshes, TF and views)",
         "config": {"workload": wl["name"], "desc": wl["desc"], "form": args.form,
-                   "tets": int(wl["tet"].shape[0]), "verts": int(wl["vert"].shape[0]),
-                   "ext_faces": int(wl["extf"].shape[0]), "views": nv,
-                   "resolution": f"{W}x{H}", "rays_per_step": rays_step,
+                   "meshes": [{"cells": p["n"], "tets": int(p["tet"].shape[0]),
+                               "verts": int(p["vert"].shape[0]),
+                               "ext_faces": int(p["extf"].shape[0])} for p in wl["meshes"]],
+                   "jobs": nj, "pixels_per_step": int(npix), "rays_per_step": rays_step,
                    "tet_steps_per_step": steps_step, "mode": "reference (last visible face wins)",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
-                   "parallelism": f"{world} replica(s), one per GPU"},
-        "fps": round(nv * world * K / (t_main * 1e-3), 2),
-        "gsteps_per_s": round(steps_step * world * K / (t_main * 1e-3) / 1e9, 3),
-        "plain_per_view": {"value": round(plain, 2), "unit": "Mrays/s",
-                           "ms_per_step": round(t_plain / max(1, min(K, 3)), 3)},
-        "e2e": {"value": round(e2e, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 64 * nv,
-                "d2h_bytes_per_step": nv * W * H * 3, "ms_per_step": round(t_e2e / K, 3)},
-        "gpu_launches": int(launches_per_step * (K)),
+                   "parallelism": f"{world} replica(s), one per GPU", "tuning": tuning},
+        "fps": round(float(nj * world * K / (t_main * 1e-3)), 2),
+        "gsteps_per_s": round(float(steps_step * world * K / (t_main * 1e-3) / 1e9), 3),
+        "batched": {"value": round(float(mrays(t_batch, kp)), 2), "unit": "Mrays/s",
+                    "ms_per_step": round(float(t_batch / kp), 3)},
+        "plain_per_view": {"value": round(float(mrays(t_plain, kp)), 2), "unit": "Mrays/s",
+                           "ms_per_step": round(float(t_plain / kp), 3)},
+        "batched_over_plain": round(float(t_plain / t_batch), 3),
+        "e2e": {"value": round(float(e2e), 2), "unit": "Mrays/s", "h2d_bytes_per_step": 64 * nj,
+                "d2h_bytes_per_step": int(npix * 3), "ms_per_step": round(float(t_e2e / K), 3)},
+        "gpu_launches": int(launches_per_step * K),
         "roofline": roof,
         "clocks": clk.summary(),
     }
     return out, wl
 
 
+# ------------------------------------------------------------------ served
+
+def run_served(args):
+    """Poisson arrivals of requests over the mixed meshes at each rate for a
+    fixed time; latency = submit to image in host memory."""
+    from vfray_b200 import serve, synth
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = make_workload("served")
+    r, stream, mids = setup_gpu(wl, dev)
+    rng = np.random.default_rng(7)
+    res = (256, 512, 1024)
+    views = synth.orbit_views(32, seed=11)
+    results = []
+    with Clocks(dev) as clk:
+        for rate in [float(x) for x in args.rates.split(",")]:
+            n = max(8, int(rate * args.served_seconds))
+            gaps = rng.exponential(1.0 / rate, size=n)
+            reqs = [(mids[int(rng.integers(len(mids)))], views[int(rng.integers(len(views)))],
+                     int(res[rng.integers(len(res))])) for _ in range(n)]
+            with serve.Server(r, budget_bytes=120 << 30) as S:
+                tickets = []
+                t0 = time.perf_counter()
+                due = t0
+                for (m, mv, s), g in zip(reqs, gaps):
+                    due += g
+                    d = due - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    tickets.append(S.submit(m, s, s, mv=mv))
+                infos = [S.wait(t, timeout_ms=600000)[1] for t in tickets]
+                t1 = time.perf_counter()
+            lat = [i["t_done_ms"] - i["t_submit_ms"] for i in infos]
+            span = max(i["t_done_ms"] for i in infos) - min(i["t_submit_ms"] for i in infos)
+            rays = sum(i["num_rays"] for i in infos)
+            results.append({"rate_req_s": rate, "requests": n,
+                            "achieved_req_s": round(n / (t1 - t0), 1),
+                            **{k: round(v, 3) for k, v in serve.percentiles(lat).items()},
+                            "mrays_s": round(rays / (span * 1e-3) / 1e6, 2),
+                            "mean_batch": round(float(np.mean([i["batch_jobs"] for i in infos])), 1)})
+    for m in mids:
+        r.release_mesh(m)
+    r.close()
+    best = max(results, key=lambda x: x["mrays_s"])
+    return {"metric": "Mrays/s + p50/p99 latency (served: Poisson arrivals over 8 carved meshes, "
+                      "256^2..1024^2 requests)", "value": best["mrays_s"], "unit": "Mrays/s",
+            "n_gpus": 1, "steps": len(results), "warmup": 0, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded meshes, TF, cameras and arrivals)",
+            "config": {"workload": "served", "rates": results, "budget_bytes": 120 << 30},
+            "clocks": clk.summary()}
+
+
 # ------------------------------------------------------------------ reference (CPU)
 
 def reference_sample(wl, seconds, threads=0):
-    """The reference's CPU kernels (oracle/_ref, its own -O3 -ffast-math
-    flags) on all host cores over the workload's views, in order, until
-    ``seconds`` have passed (at least one view).  Per view: rotateVolume,
-    normalizeVertices and buildLmt of the reference, then its three stages."""
+    """The reference's CPU kernels (oracle/_ref, its own -O3 -ffast-math flags)
+    on all host cores over the workload's jobs in order, until ``seconds``
+    have passed (at least one job).  Per job: rotateVolume, normalizeVertices
+    and buildLmt of the reference, then its three stages."""
     import oracle
 
     R = oracle.Reference("fast")
-    base = wl["vert"]
     nthreads = threads or os.cpu_count() or 1
     done = 0
     t0 = time.perf_counter()
     R.set_tf(wl["tf"])
-    for mv in wl["views"]:
-        R.set_mesh(base, wl["tet"])
+    for (m, mv, W, H) in wl["jobs"]:
+        p = wl["meshes"][m]
+        R.set_mesh(p["vert"], p["tet"])
         if mv is not None:
             R.rotate(mv)
             R.normalize()
-        R.set_con(wl["con"], wl["extf"].shape[0])
-        R.set_extf(wl["extf"])
+        R.set_con(p["con"], p["extf"].shape[0])
+        R.set_extf(p["extf"])
         R.build_lmt()
-        R.render_mt(wl["W"], wl["H"], threads=nthreads)
+        R.render_mt(W, H, threads=nthreads)
         done += 1
         if time.perf_counter() - t0 >= seconds:
             break
-    dt = time.perf_counter() - t0
-    return done, dt, nthreads
+    return done, time.perf_counter() - t0, nthreads
 
 
-def count_rays(wl):
-    """Rays (pixels with an entry face) per view, from the oracle's winner pass."""
+def count_rays(wl, njobs):
+    """Rays (pixels with an entry face) per job, from the oracle's winner pass."""
     import oracle
     import vfray_b200 as vb
 
     Or = oracle.Oracle()
     out = []
-    for mv in wl["views"]:
-        v = wl["vert"] if mv is None else vb.normalize(vb.rotate(wl["vert"], mv))
-        m = Or.mesh(v, wl["tet"], wl["con"], wl["extf"], wl["tf"], wl["psi"], wl["lmt"][0])
-        out.append(int((Or.winners(m, wl["W"], wl["H"]) >= 0).sum()))
+    for (m, mv, W, H) in wl["jobs"][:njobs]:
+        p = wl["meshes"][m]
+        v = p["vert"] if mv is None else vb.normalize(vb.rotate(p["vert"], mv))
+        om = Or.mesh(v, p["tet"], p["con"], p["extf"], wl["tf"], wl["psi"], p["lmt"][0])
+        out.append(int((Or.winners(om, W, H) >= 0).sum()))
     return out
 
 
-def cpu_baseline(wl, seconds, rays_per_view=None):
+def cpu_baseline(wl, seconds):
     done, dt, nthreads = reference_sample(wl, seconds)
-    if rays_per_view is None:
-        rays_per_view = count_rays({**wl, "views": wl["views"][:done]})
-    rays = sum(rays_per_view[:done])
+    rays = sum(count_rays(wl, done))
     return {"value": round(rays / dt / 1e6, 4), "unit": "Mrays/s", "cores": nthreads,
             "kind": "reference",
-            "sample": f"{done} of {len(wl['views'])} views, reference vfRayKernelCPU.cc "
+            "sample": f"{done} of {len(wl['jobs'])} jobs, reference vfRayKernelCPU.cc "
                       f"(-O3 -ffast-math) on {nthreads} threads (column strips), {dt:.1f} s"}
 
 
 def run_reference(args, rank):
     if rank != 0:
         return None
-    wl = make_workload(args.workload)
     import oracle
 
     if not oracle.ref_available("fast"):
         return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}
-    rays_pv = count_rays(wl)
+    wl = make_workload("mixed" if args.workload == "served" else args.workload, args.views)
     per_step_s = max(1.0, args.cpu_seconds / 4)
     for _ in range(args.warmup):
         reference_sample(wl, 0.0)
-    total_rays, total_t, nthreads, views_done = 0, 0.0, 1, 0
+    total_rays, total_t, nthreads, jobs_done = 0, 0.0, 1, 0
     for _ in range(args.steps):
         done, dt, nthreads = reference_sample(wl, per_step_s)
-        total_rays += sum(rays_pv[:done])
+        total_rays += sum(count_rays(wl, done))
         total_t += dt
-        views_done += done
+        jobs_done += done
     v = total_rays / total_t / 1e6
     return {"impl": "reference", "metric": f"Mrays/s ({wl['desc']})", "value": round(v, 4),
             "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(total_t / args.steps * 1e3, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded meshes, TF and views)",
-            "config": {"workload": wl["name"], "desc": wl["desc"], "resolution": f"{wl['W']}x{wl['H']}",
-                       "views_per_step": "bounded sample (first views of the orbit)"},
+            "config": {"workload": wl["name"], "desc": wl["desc"],
+                       "jobs_per_step": "bounded sample (the first jobs of the workload)"},
             "cpu_baseline": {"value": round(v, 4), "unit": "Mrays/s", "cores": nthreads,
                              "kind": "reference",
-                             "sample": f"{views_done} views over {args.steps} steps, reference "
+                             "sample": f"{jobs_done} jobs over {args.steps} steps, reference "
                                        f"vfRayKernelCPU.cc (-O3 -ffast-math) on {nthreads} threads"},
             "e2e": {"value": round(v, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -427,12 +527,16 @@ def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    dist = None
     if args.impl == "reference":
         out = run_reference(args, rank)
         if out is not None:
             print(_json(out))
         return
+    if args.workload == "served":
+        if rank == 0:
+            print(_json(run_served(args)))
+        return
+    dist = None
     if world > 1:
         import datetime
 

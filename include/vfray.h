@@ -56,6 +56,7 @@ extern "C" {
 #define VFR_OPT_TRAVERSE_VARIANT 5 /* traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM */
 #define VFR_OPT_REFILL 6          /* refill a warp's idle lanes once >= this many are idle (4) */
 #define VFR_OPT_RASTER_WARPS 7    /* stage (b) warps per SM (64) */
+#define VFR_OPT_TILE_WIDTH 8      /* ray-list screen tile width: 4, 8, 16, 32 (8 = 8x4) */
 
 /* Render modes. */
 #define VFR_MODE_REF 0        /* reference semantics: last visible face wins each pixel */
@@ -192,8 +193,62 @@ VFR_API int vfr_batch_output(vfr_batch* b, uint32_t job, uint8_t** rgb8_dev, flo
  * (any may be NULL), and waits: the host-buffer end of a batch. */
 VFR_API int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host,
                            uint32_t* steps_host);
+/* Autotuner: times stages (b) and (c) of the batch over a grid of the
+ * knobs above (traversal register budget, refill threshold, traversal CTAs
+ * per SM, ray-tile shape, stage (b) warps per SM), best of `reps` runs each,
+ * keeps the fastest on the context and reports it.  Drops a captured graph
+ * (capture again). */
+typedef struct {
+  uint32_t variant, refill, blocks_per_sm, tile_w, raster_warps_per_sm;
+  float ms;  /* stages (b) + (c) of the batch with these knobs */
+} vfr_tuning;
+VFR_API int vfr_batch_autotune(vfr_batch* b, int reps, vfr_tuning* out);
 /* Device bytes of the batch's scratch arenas. */
 VFR_API int vfr_batch_scratch_bytes(vfr_batch* b, uint64_t* bytes);
+
+/* ---- served form: a request loop with continuous batching -------------- */
+
+/* No counterpart in the reference.  Requests over the context's resident
+ * meshes are submitted from any thread; a worker thread admits them in
+ * arrival order while their memory footprint (the view's scratch and image
+ * buffers) fits the budget left, folds all admitted requests -- meshes and
+ * image sizes mixed -- into one batch and launches it on one of two batch
+ * slots with their own streams, so a batch formed while another runs
+ * overlaps it on the device.  A request whose footprint exceeds the whole
+ * budget is refused (VFR_ERR_BUDGET).  Upload the meshes before creating the
+ * server and release them after destroying it. */
+typedef struct {
+  int mesh_id;
+  uint32_t W, H;
+  int use_mv;
+  float mv[16];
+  int mode;             /* VFR_MODE_REF or VFR_MODE_COMPOSITED */
+  uint8_t* rgb8_host;   /* W*H*3, written before the request completes; may be NULL */
+} vfr_request;
+
+typedef struct {
+  int status;
+  double t_submit_ms, t_start_ms, t_done_ms;  /* since the server started */
+  uint32_t batch_id, batch_jobs;               /* the batch it ran in, its size */
+  uint32_t num_rays;
+  uint64_t num_steps;
+} vfr_request_info;
+
+typedef struct {
+  uint32_t batches, pending;
+  uint64_t completed, rejected, budget_used, rays, steps;
+} vfr_server_counters;
+
+typedef struct vfr_server vfr_server;
+VFR_API int vfr_server_create(vfr_ctx* ctx, uint64_t budget_bytes, uint32_t max_batch,
+                              vfr_server** out);
+VFR_API int vfr_server_submit(vfr_server* s, const vfr_request* r, uint64_t* ticket);
+/* Waits for a request (timeout_ms < 0: no limit; VFR_ERR_TIMEOUT if it runs
+ * out), fills info, forgets the ticket; returns the request's status. */
+VFR_API int vfr_server_wait(vfr_server* s, uint64_t ticket, int timeout_ms, vfr_request_info* info);
+VFR_API int vfr_server_stats(vfr_server* s, vfr_server_counters* out);
+/* Drains the admitted and pending requests, then stops. */
+VFR_API void vfr_server_destroy(vfr_server* s);
 
 /* ---- stage (a) for callers that cannot allocate ------------------------ */
 

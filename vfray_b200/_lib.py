@@ -38,6 +38,7 @@ OPT_PROFILE = 4
 OPT_TRAVERSE_VARIANT = 5
 OPT_REFILL = 6
 OPT_RASTER_WARPS = 7
+OPT_TILE_WIDTH = 8
 
 MODE_REF = 0
 MODE_COMPOSITED = 1
@@ -64,6 +65,41 @@ class Job(C.Structure):
     _fields_ = [("mesh_id", C.c_int), ("W", C.c_uint32), ("H", C.c_uint32), ("use_mv", C.c_int),
                 ("mv", C.c_float * 16), ("rgb8_dev", C.c_void_p), ("rgba_dev", C.c_void_p),
                 ("steps_dev", C.c_void_p)]
+
+
+class Tuning(C.Structure):
+    """vfr_tuning of include/vfray.h."""
+    _fields_ = [("variant", C.c_uint32), ("refill", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("tile_w", C.c_uint32), ("raster_warps_per_sm", C.c_uint32), ("ms", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Request(C.Structure):
+    """vfr_request of include/vfray.h."""
+    _fields_ = [("mesh_id", C.c_int), ("W", C.c_uint32), ("H", C.c_uint32), ("use_mv", C.c_int),
+                ("mv", C.c_float * 16), ("mode", C.c_int), ("rgb8_host", C.c_void_p)]
+
+
+class RequestInfo(C.Structure):
+    """vfr_request_info of include/vfray.h."""
+    _fields_ = [("status", C.c_int), ("t_submit_ms", C.c_double), ("t_start_ms", C.c_double),
+                ("t_done_ms", C.c_double), ("batch_id", C.c_uint32), ("batch_jobs", C.c_uint32),
+                ("num_rays", C.c_uint32), ("num_steps", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    """vfr_server_stats of include/vfray.h."""
+    _fields_ = [("batches", C.c_uint32), ("pending", C.c_uint32), ("completed", C.c_uint64),
+                ("rejected", C.c_uint64), ("budget_used", C.c_uint64), ("rays", C.c_uint64),
+                ("steps", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _vp = C.c_void_p
@@ -100,7 +136,13 @@ SIGNATURES = {
     "vfr_batch_stats": (_i, [_vp, C.POINTER(RenderStats), _u32]),
     "vfr_batch_output": (_i, [_vp, _u32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
     "vfr_batch_read": (_i, [_vp, _vp, _vp, _vp]),
+    "vfr_batch_autotune": (_i, [_vp, _i, C.POINTER(Tuning)]),
     "vfr_batch_scratch_bytes": (_i, [_vp, C.POINTER(C.c_uint64)]),
+    "vfr_server_create": (_i, [_vp, C.c_uint64, _u32, C.POINTER(_vp)]),
+    "vfr_server_submit": (_i, [_vp, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "vfr_server_wait": (_i, [_vp, C.c_uint64, _i, C.POINTER(RequestInfo)]),
+    "vfr_server_stats": (_i, [_vp, C.POINTER(ServerStats)]),
+    "vfr_server_destroy": (None, [_vp]),
     "vfr_find_visible_static": (_i, [_vp, _u32, _vp, _u32, _vp, _u32, _vp, _vp, _vp]),
     "vfr_psi_table": (_i, [_vp]),
     "vfr_normalize": (_i, [_vp, _u32]),

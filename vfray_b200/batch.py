@@ -9,7 +9,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import Job, RenderStats, check, ptr
+from ._lib import Job, RenderStats, Tuning, check, ptr
 
 __all__ = ["BatchRenderer", "job"]
 
@@ -55,6 +55,16 @@ class BatchRenderer:
         check(self.lib.vfr_batch_set_jobs(self.h, arr, len(js), self.mode), self.r.h,
               "vfr_batch_set_jobs")
         self.captured = False
+
+    def autotune(self, reps: int = 2) -> dict:
+        """Pick the fastest knobs for this batch (kept on the renderer's
+        context) and re-capture the graph."""
+        t = Tuning()
+        check(self.lib.vfr_batch_autotune(self.h, reps, C.byref(t)), self.r.h,
+              "vfr_batch_autotune")
+        self.captured = False
+        self.prepare()
+        return t.as_dict()
 
     def prepare(self):
         """Capture the chain as a CUDA graph (once)."""

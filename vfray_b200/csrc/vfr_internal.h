@@ -8,7 +8,7 @@
 #include <vector>
 
 #include "vfr_host.h"
-#include "vfr_traverse.cuh"
+#include "vfr_types.cuh"
 
 namespace vfr {
 
@@ -50,6 +50,7 @@ struct Tuning {
   uint32_t refill = 4;         // refill idle lanes once this many of a warp's are idle
   uint32_t variant = 0;        // traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM
   uint32_t raster_warps_per_sm = 64;
+  uint32_t tile_w = 8;          // ray-list tile width (x 32/tile_w rows)
 };
 
 struct Ctx;
@@ -83,6 +84,8 @@ struct Batch {
   Buf out_rgb8, out_rgba, out_steps;      // outputs owned by the batch (host-output calls)
   size_t ent_cap = 0;
   cudaGraphExec_t exec = nullptr;
+  cudaStream_t stream = nullptr;  // null: the context's stream
+  cudaStream_t st() const;
   // pinned staging for the per-call upload of a one-job batch
   void* stage = nullptr;
   size_t stage_cap = 0;
@@ -92,6 +95,7 @@ struct Batch {
   uint32_t* vis_pref() const { return d_dev_pref.as<uint32_t>(); }
   uint32_t* ray_pref() const { return d_dev_pref.as<uint32_t>((njobs + 1) * 4); }
   uint32_t* queue() const { return d_dev_pref.as<uint32_t>(2 * (njobs + 1) * 4); }
+  uint32_t tile_w = 8;  // the tile shape the layout was made for
   int layout(const std::vector<JobSpec>& s, int mode, bool own_outputs);
   int upload(bool async);
   int enqueue_a();
@@ -144,3 +148,8 @@ struct Ctx {
 };
 
 }  // namespace vfr
+
+// The C ABI's context handle.
+struct vfr_ctx {
+  vfr::Ctx impl;
+};

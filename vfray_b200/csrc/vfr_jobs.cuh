@@ -9,49 +9,9 @@
 // prefix_kernel.  Nothing waits on the host between stages, so a batch is one
 // stream-ordered chain of launches (and can be captured as a CUDA graph).
 #pragma once
-#include "vfr_device.cuh"
+#include "vfr_types.cuh"
 
 namespace vfr {
-
-// Per-view device counters.
-struct __align__(16) ViewCounters {
-  uint32_t nvis;             // visible faces
-  uint32_t nrays;            // rays of this job
-  uint32_t nentries;         // entry-list entries (composited mode)
-  uint32_t status;           // VFR_DEV_* bits
-  unsigned long long steps;  // tet-walk iterations of this job's rays
-  uint32_t maxedge_bits;     // view maxEdgeLength (float bits, >= 0)
-  uint32_t pad;
-  uint32_t mm[8];            // orderable min x y z s, max x y z s (view set-up)
-};
-
-// One job as the kernels see it (device memory, uploaded with the batch).
-struct __align__(16) JobDev {
-  float4 m0, m1, m2;         // rows of the model-view (use_mv)
-  const uint4* tet;          // mesh
-  const WalkRec* walk;
-  const float4* vert_in;     // the mesh's (normalised) vertices
-  const uint2* extf;
-  const float4* vert;        // vertices this view renders with (vert_in or vview)
-  float4* vview;             // rotated + normalised vertices (use_mv)
-  float4* planes;            // 2 per external face
-  uint32_t* blk;             // visible count per block of 1024 external faces
-  uint32_t* vis_ext;         // visible external faces, in order
-  uint4* bbox;               // per visible face
-  int32_t* winner;           // W*H, reference mode
-  uint32_t* rays;            // W*H capacity
-  uint32_t* ent_cnt;         // composited: W*H counts (batch arena)
-  uint32_t* ent_off;         // composited: offsets (batch arena, global)
-  uint32_t* ent_cur;
-  ViewCounters* ctr;
-  uint8_t* rgb8;             // outputs (any may be null)
-  float4* rgba;
-  uint32_t* steps;
-  uint32_t nV, nT, nExt, W, H;
-  uint32_t use_mv;
-  float maxEdge_in;          // the mesh's maxEdgeLength when !use_mv
-  uint32_t pix_base;         // first pixel of this job in the batch's pixel arenas
-};
 
 // Largest j with pref[j] <= g (pref[0] = 0, pref has n+1 entries, g < pref[n]).
 __device__ __forceinline__ uint32_t job_of(const uint32_t* __restrict__ pref, uint32_t n, uint32_t g) {
@@ -377,21 +337,23 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
   }
 }
 
-// Ray lists: the pixels with an entry face, in 8x4 screen tiles (one warp per
-// tile, tiles of all jobs in one index space) so that neighbouring rays,
-// which walk neighbouring tets, are neighbours in the list.  Pixels without
-// one are cleared in the outputs here (the reference zero-fills its image,
-// main.cc:194).
+// Ray lists: the pixels with an entry face, in screen tiles of 32 pixels
+// (tw x 32/tw, one warp per tile, tiles of all jobs in one index space) so
+// that neighbouring rays, which walk neighbouring tets, are neighbours in the
+// list and share warps.  Pixels without one are cleared in the outputs here
+// (the reference zero-fills its image, main.cc:194).
 __global__ void __launch_bounds__(256) raylist_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
-                                                      const uint32_t* __restrict__ tpref, int mode) {
+                                                      const uint32_t* __restrict__ tpref, int mode,
+                                                      uint32_t tw) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (g >= tpref[njobs]) return;
   const uint32_t j = job_of(tpref, njobs, g);
   const JobDev& J = jobs[j];
   const uint32_t tile = g - tpref[j];
-  const uint32_t tx = (J.W + 7) >> 3;
-  const uint32_t x = (tile % tx) * 8 + (lane & 7), y = (tile / tx) * 4 + (lane >> 3);
+  const uint32_t th = 32u / tw;
+  const uint32_t tx = (J.W + tw - 1) / tw;
+  const uint32_t x = (tile % tx) * tw + (lane % tw), y = (tile / tx) * th + (lane / tw);
   bool has = false;
   uint32_t p = 0;
   const bool inside = x < J.W && y < J.H;

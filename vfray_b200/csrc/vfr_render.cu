@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "vfr_internal.h"
+#include "vfr_traverse.cuh"
 #include "vfray.h"
 
 namespace vfr {
@@ -69,7 +70,7 @@ int Ctx::grow(Buf& b, size_t bytes, const char* what) {
   if (bytes == 0) bytes = 16;
   if (b.cap >= bytes && b.p) return VFR_OK;
   if (b.p) {
-    cudaStreamSynchronize(stream);  // in-flight work may still use the old buffer
+    cudaDeviceSynchronize();  // in-flight work (any stream) may still use the old buffer
     cudaFree(b.p);
   }
   b.p = nullptr;
@@ -137,6 +138,8 @@ Batch::~Batch() {
   if (stage_done) cudaEventDestroy(stage_done);
 }
 
+cudaStream_t Batch::st() const { return stream ? stream : ctx->stream; }
+
 void Batch::drop_graph() {
   if (exec) cudaGraphExecDestroy(exec);
   exec = nullptr;
@@ -150,6 +153,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
   Ctx& C = *ctx;
   specs = s;
   mode = m;
+  tile_w = C.tune.tile_w;
   njobs = (uint32_t)s.size();
   jobs.assign(njobs, JobDev{});
   pref.assign(4 * (size_t)(njobs + 1), 0);
@@ -169,7 +173,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     const uint32_t eb =
         q.use_mv ? std::max<uint32_t>(1, std::min<uint32_t>(cdiv(mesh->nT, 1024), 4 * C.num_sms)) : 0;
     const uint32_t xb = cdiv(mesh->nExt, 1024);
-    const uint32_t tl = cdiv(q.W, 8) * cdiv(q.H, 4);
+    const uint32_t tl = cdiv(q.W, C.tune.tile_w) * cdiv(q.H, 32 / C.tune.tile_w);
     pr[j + 1] = pr[j] + rb;
     pe[j + 1] = pe[j] + eb;
     px[j + 1] = px[j] + xb;
@@ -272,12 +276,12 @@ int Batch::upload(bool async) {
   Ctx& C = *ctx;
   const size_t bj = sizeof(JobDev) * njobs, bp = sizeof(uint32_t) * pref.size();
   if (!async) {
-    int rc = C.cuda(cudaMemcpyAsync(d_jobs.p, jobs.data(), bj, cudaMemcpyHostToDevice, C.stream),
+    int rc = C.cuda(cudaMemcpyAsync(d_jobs.p, jobs.data(), bj, cudaMemcpyHostToDevice, st()),
                     "job table upload");
     if (!rc)
-      rc = C.cuda(cudaMemcpyAsync(d_pref.p, pref.data(), bp, cudaMemcpyHostToDevice, C.stream),
+      rc = C.cuda(cudaMemcpyAsync(d_pref.p, pref.data(), bp, cudaMemcpyHostToDevice, st()),
                   "prefix upload");
-    if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "upload");
+    if (!rc) rc = C.cuda(cudaStreamSynchronize(st()), "upload");
     return rc;
   }
   if (!stage_done) cudaEventCreateWithFlags(&stage_done, cudaEventDisableTiming);
@@ -292,18 +296,18 @@ int Batch::upload(bool async) {
   cudaEventSynchronize(stage_done);
   std::memcpy(stage, jobs.data(), bj);
   std::memcpy((char*)stage + bj, pref.data(), bp);
-  int rc = C.cuda(cudaMemcpyAsync(d_jobs.p, stage, bj, cudaMemcpyHostToDevice, C.stream),
+  int rc = C.cuda(cudaMemcpyAsync(d_jobs.p, stage, bj, cudaMemcpyHostToDevice, st()),
                   "job table upload");
   if (!rc)
-    rc = C.cuda(cudaMemcpyAsync(d_pref.p, (char*)stage + bj, bp, cudaMemcpyHostToDevice, C.stream),
+    rc = C.cuda(cudaMemcpyAsync(d_pref.p, (char*)stage + bj, bp, cudaMemcpyHostToDevice, st()),
                 "prefix upload");
-  cudaEventRecord(stage_done, C.stream);
+  cudaEventRecord(stage_done, st());
   return rc;
 }
 
 int Batch::enqueue_a() {
   Ctx& C = *ctx;
-  cudaStream_t st = C.stream;
+  const cudaStream_t st = Batch::st();
   const JobDev* J = d_jobs.as<JobDev>();
   const uint32_t* P = d_pref.as<uint32_t>();
   const uint32_t n1 = njobs + 1;
@@ -323,7 +327,7 @@ int Batch::enqueue_a() {
 
 int Batch::enqueue_b() {
   Ctx& C = *ctx;
-  cudaStream_t st = C.stream;
+  const cudaStream_t st = Batch::st();
   const JobDev* J = d_jobs.as<JobDev>();
   const uint32_t* P = d_pref.as<uint32_t>();
   const uint32_t n1 = njobs + 1;
@@ -343,7 +347,7 @@ int Batch::enqueue_b() {
                                                    (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu));
     entry_totals_kernel<<<cdiv(njobs, 128), 128, 0, st>>>(J, njobs);
   }
-  if (tiles) raylist_kernel<<<cdiv(tiles, 8), 256, 0, st>>>(J, njobs, P + 3 * n1, mode);
+  if (tiles) raylist_kernel<<<cdiv(tiles, 8), 256, 0, st>>>(J, njobs, P + 3 * n1, mode, tile_w);
   prefix_kernel<<<1, 1024, 0, st>>>(J, njobs, 1, ray_pref());
   return C.cuda(cudaGetLastError(), "stage (b) launch");
 }
@@ -365,7 +369,7 @@ int Batch::enqueue_c() {
   const int blocks = C.num_sms * C.traverse_blocks_per_sm(mode);
   void* args[] = {&P};
   return C.cuda(cudaLaunchKernel(C.traverse_fn(mode, C.tune.variant), dim3(blocks), dim3(256), args,
-                                 0, C.stream),
+                                 0, st()),
                 "stage (c) launch");
 }
 
@@ -373,10 +377,10 @@ int Batch::capture() {
   Ctx& C = *ctx;
   drop_graph();
   cudaGraph_t g = nullptr;
-  int rc = C.cuda(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal), "capture");
+  int rc = C.cuda(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal), "capture");
   if (rc) return rc;
   rc = enqueue_all();
-  cudaError_t e = cudaStreamEndCapture(C.stream, &g);
+  cudaError_t e = cudaStreamEndCapture(st(), &g);
   if (!rc) rc = C.cuda(e, "end capture");
   if (!rc) rc = C.cuda(cudaGraphInstantiate(&exec, g, 0), "graph instantiate");
   if (g) cudaGraphDestroy(g);
@@ -385,7 +389,7 @@ int Batch::capture() {
 }
 
 int Batch::run() {
-  if (exec) return ctx->cuda(cudaGraphLaunch(exec, ctx->stream), "graph launch");
+  if (exec) return ctx->cuda(cudaGraphLaunch(exec, st()), "graph launch");
   return enqueue_all();
 }
 
@@ -393,9 +397,9 @@ int Batch::counters(std::vector<ViewCounters>& out) {
   Ctx& C = *ctx;
   out.resize(njobs);
   int rc = C.cuda(cudaMemcpyAsync(out.data(), d_ctr.p, sizeof(ViewCounters) * njobs,
-                                  cudaMemcpyDeviceToHost, C.stream),
+                                  cudaMemcpyDeviceToHost, st()),
                   "counter read");
-  if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "stream sync");
+  if (!rc) rc = C.cuda(cudaStreamSynchronize(st()), "stream sync");
   return rc;
 }
 
@@ -405,10 +409,6 @@ using vfr::Batch;
 using vfr::Ctx;
 using vfr::JobSpec;
 using vfr::Mesh;
-
-struct vfr_ctx {
-  Ctx impl;
-};
 
 struct vfr_batch {
   vfr_ctx* owner = nullptr;
@@ -542,6 +542,11 @@ int vfr_set_option(vfr_ctx* c, int option, int64_t value) {
     case VFR_OPT_REFILL:
       if (value < 1 || value > 32) return C.fail(VFR_ERR_INVALID, "refill is 1..32");
       C.tune.refill = (uint32_t)value;
+      return VFR_OK;
+    case VFR_OPT_TILE_WIDTH:
+      if (value != 4 && value != 8 && value != 16 && value != 32)
+        return C.fail(VFR_ERR_INVALID, "tile width is 4, 8, 16 or 32");
+      C.tune.tile_w = (uint32_t)value;
       return VFR_OK;
     case VFR_OPT_RASTER_WARPS:
       if (value < 1 || value > 64) return C.fail(VFR_ERR_INVALID, "raster warps per SM is 1..64");
@@ -936,6 +941,86 @@ int vfr_batch_output(vfr_batch* b, uint32_t job, uint8_t** rgb8_dev, float** rgb
   if (rgba_dev) *rgba_dev = (float*)b->b.specs[job].rgba;
   if (steps_dev) *steps_dev = b->b.specs[job].steps;
   return VFR_OK;
+}
+
+// Autotuner: times stages (b) and (c) of the batch (direct launches, events
+// on the context stream, best of `reps`) over a grid of the knobs --
+// traversal register budget, refill threshold, traversal CTAs per SM, ray
+// tile shape, stage (b) warps per SM -- and keeps the fastest on the context.
+int vfr_batch_autotune(vfr_batch* b, int reps, vfr_tuning* out) {
+  if (!b || !b->b.njobs) return VFR_ERR_STATE;
+  if (!b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  if (!C.d_tf) return C.fail(VFR_ERR_STATE, "tables not uploaded");
+  if (reps < 1) reps = 1;
+  const vfr::Tuning saved = C.tune;
+  const std::vector<JobSpec> specs = b->b.specs;
+  const int mode = b->b.mode;
+  cudaEvent_t e0, e1, e2;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventCreate(&e2);
+  int occ_max = 0;
+  vfr::Tuning best = saved;
+  float best_ms = 1e30f;
+  int rc = VFR_OK;
+  const uint32_t variants[] = {0, 1}, refills[] = {1, 4}, tiles[] = {4, 8, 16},
+                 rasters[] = {16, 64};
+  for (uint32_t var : variants)
+    for (uint32_t rf : refills)
+      for (uint32_t tw : tiles)
+        for (uint32_t rw : rasters)
+          for (int bsm = 0; bsm < 2 && !rc; ++bsm) {
+            vfr::Tuning t = saved;
+            t.variant = var;
+            t.refill = rf;
+            t.tile_w = tw;
+            t.raster_warps_per_sm = rw;
+            t.blocks_per_sm = 0;
+            C.tune = t;
+            if (bsm) {
+              occ_max = C.traverse_blocks_per_sm(mode);
+              if (occ_max < 2) continue;
+              C.tune.blocks_per_sm = occ_max - 1;
+            }
+            rc = b->b.layout(specs, mode, false);
+            if (!rc) rc = b->b.upload(false);
+            float ms = 1e30f;
+            for (int r = 0; r < reps + 1 && !rc; ++r) {
+              rc = b->b.enqueue_a();
+              cudaEventRecord(e0, C.stream);
+              if (!rc) rc = b->b.enqueue_b();
+              cudaEventRecord(e1, C.stream);
+              if (!rc) rc = b->b.enqueue_c();
+              cudaEventRecord(e2, C.stream);
+              if (!rc) rc = C.cuda(cudaEventSynchronize(e2), "autotune");
+              float m = 0;
+              cudaEventElapsedTime(&m, e0, e2);
+              if (r > 0) ms = std::min(ms, m);  // the first run warms up
+            }
+            if (!rc && ms < best_ms) {
+              best_ms = ms;
+              best = C.tune;
+            }
+          }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  C.tune = rc ? saved : best;
+  int rc2 = b->b.layout(specs, mode, false);
+  if (!rc2) rc2 = b->b.upload(false);
+  b->b.drop_graph();
+  if (rc) return rc;
+  if (out) {
+    out->variant = best.variant;
+    out->refill = best.refill;
+    out->blocks_per_sm = best.blocks_per_sm;
+    out->tile_w = best.tile_w;
+    out->raster_warps_per_sm = best.raster_warps_per_sm;
+    out->ms = best_ms;
+  }
+  return rc2;
 }
 
 int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host, uint32_t* steps_host) {

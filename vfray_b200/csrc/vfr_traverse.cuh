@@ -16,20 +16,6 @@
 
 namespace vfr {
 
-struct TraverseParams {
-  const JobDev* jobs;
-  uint32_t njobs;
-  const uint32_t* ray_pref;  // njobs + 1, exclusive prefix of the jobs' ray counts
-  uint32_t* queue;           // work-queue head over all jobs' rays
-  const uint2* ent;          // composited: entry arena (z bits, ext face)
-  uint32_t ent_cap;
-  const float4* tf;          // 256 RGBA
-  const float* psi;          // 512 x 512
-  uint32_t psi_one;          // psi[0][0] == 1 (zero-extinction shortcut allowed)
-  uint32_t step_cap;         // 0: 4 * nT + 64 of each job's mesh
-  uint32_t refill;           // refill a warp's idle lanes once this many are idle
-};
-
 // One exit candidate (vfRayKernelCPU.cc:312-348), branch-free.  The slack
 // test (double)(c1+c2) <= (double)cr + 1e-12 is decided in float unless cr is
 // below 2^-16: for larger cr the next float above cr is more than 1e-12 away.

@@ -1,0 +1,62 @@
+// Device-side types shared by the kernels and the host code of the render
+// library: per-view counters and the job table entry.
+#pragma once
+#include "vfr_device.cuh"
+
+namespace vfr {
+
+// Per-view device counters.
+struct __align__(16) ViewCounters {
+  uint32_t nvis;             // visible faces
+  uint32_t nrays;            // rays of this job
+  uint32_t nentries;         // entry-list entries (composited mode)
+  uint32_t status;           // VFR_DEV_* bits
+  unsigned long long steps;  // tet-walk iterations of this job's rays
+  uint32_t maxedge_bits;     // view maxEdgeLength (float bits, >= 0)
+  uint32_t pad;
+  uint32_t mm[8];            // orderable min x y z s, max x y z s (view set-up)
+};
+
+// One job as the kernels see it (device memory, uploaded with the batch).
+struct __align__(16) JobDev {
+  float4 m0, m1, m2;         // rows of the model-view (use_mv)
+  const uint4* tet;          // mesh
+  const WalkRec* walk;
+  const float4* vert_in;     // the mesh's (normalised) vertices
+  const uint2* extf;
+  const float4* vert;        // vertices this view renders with (vert_in or vview)
+  float4* vview;             // rotated + normalised vertices (use_mv)
+  float4* planes;            // 2 per external face
+  uint32_t* blk;             // visible count per block of 1024 external faces
+  uint32_t* vis_ext;         // visible external faces, in order
+  uint4* bbox;               // per visible face
+  int32_t* winner;           // W*H, reference mode
+  uint32_t* rays;            // W*H capacity
+  uint32_t* ent_cnt;         // composited: W*H counts (batch arena)
+  uint32_t* ent_off;         // composited: offsets (batch arena, global)
+  uint32_t* ent_cur;
+  ViewCounters* ctr;
+  uint8_t* rgb8;             // outputs (any may be null)
+  float4* rgba;
+  uint32_t* steps;
+  uint32_t nV, nT, nExt, W, H;
+  uint32_t use_mv;
+  float maxEdge_in;          // the mesh's maxEdgeLength when !use_mv
+  uint32_t pix_base;         // first pixel of this job in the batch's pixel arenas
+};
+
+struct TraverseParams {
+  const JobDev* jobs;
+  uint32_t njobs;
+  const uint32_t* ray_pref;  // njobs + 1, exclusive prefix of the jobs' ray counts
+  uint32_t* queue;           // work-queue head over all jobs' rays
+  const uint2* ent;          // composited: entry arena (z bits, ext face)
+  uint32_t ent_cap;
+  const float4* tf;          // 256 RGBA
+  const float* psi;          // 512 x 512
+  uint32_t psi_one;          // psi[0][0] == 1 (zero-extinction shortcut allowed)
+  uint32_t step_cap;         // 0: 4 * nT + 64 of each job's mesh
+  uint32_t refill;           // refill a warp's idle lanes once this many are idle
+};
+
+}  // namespace vfr
