@@ -273,12 +273,18 @@ __global__ void __launch_bounds__(1024) prefix_kernel(const JobDev* __restrict__
 
 // projectVisibleFaces (vfRayKernelCPU.cc:136-169) + the pixel coverage of
 // vfRay's face loop (:248-274): persistent warps over the visible faces of
-// all jobs, one warp per face, one lane per bounding-box column, y ascending;
-// an out-of-range entry scalar ends the column (:274).  The reference lets
-// the last visible face in order write a pixel; visible order is ext-face
-// order, so the winner is the largest ext-face index reaching it: atomicMax.
-// Pixels outside the image are clipped (the reference would write past its
-// buffer there).  kCount/kFill: the composited mode's entry-list passes.
+// all jobs, one warp per face, its lanes over the pixels of the face's
+// bounding box in chunks of rh rows x (32 / rh) columns (rh = the box height
+// rounded up to a power of two, at most 32).  The reference walks a column
+// y-ascending and stops it at the first covered pixel whose entry scalar is
+// out of [0,1] (:274); here the lanes of a column ballot that condition and a
+// pixel is dropped if it or a pixel above it in its column has it (carried
+// across row chunks of taller boxes).  The reference lets the last visible
+// face in order write a pixel; visible order is ext-face order, so the
+// winner is the largest ext-face index reaching it: atomicMax.  Pixels
+// outside the image are clipped (the reference would write past its buffer
+// there).  kCount/kFill: the composited mode's entry-list passes, which
+// skip only the pixel itself.
 template <bool kCount, bool kFill>
 __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
                                                      const uint32_t* __restrict__ vpref,
@@ -312,25 +318,42 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
     if (bx > xe || by > ye) continue;  // box entirely outside the image
     const EntryEdges E = entry_edges(v0, v1, v2);
     const float4 p0 = J.planes[2 * (size_t)e], p1 = J.planes[2 * (size_t)e + 1];
-    for (uint32_t px = bx + lane; px <= xe; px += 32) {
+    const uint32_t h = ye - by + 1;
+    const uint32_t rh = h >= 32 ? 32u : (h <= 1 ? 1u : 1u << (32 - __clz(h - 1)));
+    const uint32_t cw = 32u / rh;
+    const uint32_t r = lane % rh, c = lane / rh;
+    const uint32_t seg = (rh == 32 ? 0xffffffffu : ((1u << rh) - 1u)) << (c * rh);  // my column
+    const uint32_t upto = seg & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u));   // rows <= mine
+    for (uint32_t x0 = bx; x0 <= xe; x0 += cw) {
+      const uint32_t px = x0 + c;
       const float ox = obj_coord(px, W);
-      for (uint32_t py = by; py <= ye; ++py) {
-        const float oy = obj_coord(py, H);
-        if (!entry_inside(E, ox, oy)) continue;
-        const float sp = plane_eval(ox, oy, p0.w, p1.x, p1.y);
+      bool carried = false;  // a kill in an earlier row chunk of this column (rh == 32)
+      for (uint32_t y0 = by; y0 <= ye; y0 += rh) {
+        const uint32_t py = y0 + r;
+        const bool live = px <= xe && py <= ye;
+        bool inside = false, ok = false;
+        float oy = 0.0f, sp = 0.0f;
+        if (live) {
+          oy = obj_coord(py, H);
+          inside = entry_inside(E, ox, oy);
+          sp = plane_eval(ox, oy, p0.w, p1.x, p1.y);
+          ok = (sp >= 0.0f) && (sp <= 1.0f);
+        }
         const uint32_t p = py * W + px;
         if (kCount || kFill) {
-          if ((sp < 0.0f) || (sp > 1.0f)) continue;  // composited: only this pixel
-          if (kCount) {
-            atomicAdd(&J.ent_cnt[p], 1u);
-          } else {
-            const float zp = plane_eval(ox, oy, p0.x, p0.y, p0.z);
-            const uint32_t slot = J.ent_off[p] + atomicAdd(&J.ent_cur[p], 1u);
-            if (slot < ent_cap) ent[slot] = make_uint2(__float_as_uint(zp), e);
+          if (live && inside && ok) {
+            if (kCount) {
+              atomicAdd(&J.ent_cnt[p], 1u);
+            } else {
+              const float zp = plane_eval(ox, oy, p0.x, p0.y, p0.z);
+              const uint32_t slot = J.ent_off[p] + atomicAdd(&J.ent_cur[p], 1u);
+              if (slot < ent_cap) ent[slot] = make_uint2(__float_as_uint(zp), e);
+            }
           }
         } else {
-          if ((sp < 0.0f) || (sp > 1.0f)) break;  // :274 rest of the column
-          atomicMax(&J.winner[p], (int32_t)e);
+          const uint32_t kill = __ballot_sync(0xffffffffu, live && inside && !ok);
+          if (live && inside && ok && !carried && !(kill & upto)) atomicMax(&J.winner[p], (int32_t)e);
+          carried = carried || (kill & seg);
         }
       }
     }
