@@ -120,7 +120,6 @@ struct Ctx {
   std::string err;
   float4* d_tf = nullptr;
   float* d_psi = nullptr;
-  bool psi_one = false;  // psi[0][0] == 1.0f
   std::vector<std::unique_ptr<Mesh>> meshes;
   Batch plain;     // the one-job batch behind the single-view calls
   int stage = 0;   // single-view stage calls: 0 none, 1 visible done, 2 project done

@@ -363,7 +363,6 @@ int Batch::enqueue_c() {
   P.ent_cap = (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu);
   P.tf = C.d_tf;
   P.psi = C.d_psi;
-  P.psi_one = C.psi_one ? 1u : 0u;
   P.step_cap = C.step_cap;
   P.refill = C.tune.refill;
   const int blocks = C.num_sms * C.traverse_blocks_per_sm(mode);
@@ -589,7 +588,6 @@ int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
     if (rc) return rc;
   }
   cudaStreamSynchronize(C.stream);
-  C.psi_one = psi[0] == 1.0f;
   int rc = C.cuda(cudaMemcpy(C.d_tf, tf, sizeof(float) * 1024, cudaMemcpyHostToDevice), "tf upload");
   if (!rc)
     rc = C.cuda(cudaMemcpy(C.d_psi, psi, sizeof(float) * 512 * 512, cudaMemcpyHostToDevice),

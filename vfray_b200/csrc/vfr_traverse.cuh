@@ -132,8 +132,7 @@ __device__ __forceinline__ void finish_pixel(const JobDev& J, const Ray& R) {
 enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kAbandon = 2, kCap = 3, kRange = 4 };
 
 // One iteration of the reference's while loop (:302-542).
-__device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* s_tf, bool psi_one,
-                                         Ray& R) {
+__device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* s_tf, Ray& R) {
   if (++R.iters > R.cap) return kCap;
   const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
@@ -167,10 +166,7 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* 
   dz = (dz == 0.0f) ? 0.0f : fdiv(dz, R.maxEdge);
   const float4 cf = s_tf[(uint32_t)fmul(255.0f, sn)];
   const float taux = fmul(cf.w, dz), tauy = fmul(R.cb.w, dz);
-  if (!(psi_one && taux == 0.0f && tauy == 0.0f)) {
-    // With both extinctions 0: zeta = 1, gamma = 0, psi = table[0][0] = 1,
-    // so the colour term is 0 and 1 - alpha = 1: the sum is unchanged, and
-    // the step can skip to the colour hand-over (psi_one: table[0][0] == 1).
+  {
     const float zeta = (float)exp(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)));
     // tau / (1.0 + tau) in double; a zero numerator is taken apart so that
     // the division never meets its special-case path
@@ -254,7 +250,6 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
   const uint32_t lt_mask = (1u << lane) - 1u;
   const uint32_t nrays = P.ray_pref[P.njobs];
   const uint32_t refill = P.refill ? P.refill : 1u;
-  const bool psi_one = P.psi_one != 0;
   Tally T = {0xffffffffu, 0ull, 0u};
   bool active = false, exhausted = false;
   Ray R;
@@ -316,7 +311,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
       continue;
     }
     if (!active) continue;
-    const uint32_t res = step(P, s_tf, psi_one, R);
+    const uint32_t res = step(P, s_tf, R);
     if (res == kContinue) continue;
     if (res == kSegmentEnd) {
       if (kMode == 1) {

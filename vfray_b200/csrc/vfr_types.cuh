@@ -54,7 +54,6 @@ struct TraverseParams {
   uint32_t ent_cap;
   const float4* tf;          // 256 RGBA
   const float* psi;          // 512 x 512
-  uint32_t psi_one;          // psi[0][0] == 1 (zero-extinction shortcut allowed)
   uint32_t step_cap;         // 0: 4 * nT + 64 of each job's mesh
   uint32_t refill;           // refill a warp's idle lanes once this many are idle
 };
