@@ -1,0 +1,93 @@
+"""CPU checks of the exact substitutions the traversal kernel makes for the
+reference's double-precision expressions (vfRayKernelCPU.cc), restated in
+numpy: each substitution must give the reference's decision on every input
+it accepts.
+
+* exit-test slack (:341-342): (double)s <= (double)cr + 1e-12 for floats
+  s, cr with cr >= 0x2b8cbccd  <=>  float(s - cr) <= 0x2b8cbccc;
+* psi coordinate (:462-471): the float bracket around gamma = tau/(1.0+tau)
+  selects the reference's table coordinate whenever its two ends agree, for
+  any quotient estimate within the 2-ulp bound of __fdividef.
+"""
+import numpy as np
+
+F32 = np.float32
+R = 1e-12
+TH = np.array([0x2b8cbccc], np.uint32).view(F32)[0]  # largest float below 1e-12
+CRMIN = np.array([0x2b8cbccd], np.uint32).view(F32)[0]
+
+
+def test_slack_identity_near_the_threshold():
+    rng = np.random.default_rng(7)
+    bad = tot = 0
+    for _ in range(8):
+        cr = np.maximum((2.0 ** rng.uniform(-40, 20, 250_000)).astype(F32), CRMIN)
+        ulp = np.spacing(cr).astype(np.float64)
+        j0 = np.floor(R / ulp)
+        for dj in (-2, -1, 0, 1, 2, 3):
+            s = (cr.astype(np.float64) + np.maximum(j0 + dj, 0) * ulp).astype(F32)
+            ref = s.astype(np.float64) <= cr.astype(np.float64) + R
+            new = (s - cr) <= TH
+            bad += int(np.count_nonzero(ref != new))
+            tot += s.size
+        s = (cr * rng.uniform(0.0, 3.0, cr.size)).astype(F32)
+        ref = s.astype(np.float64) <= cr.astype(np.float64) + R
+        bad += int(np.count_nonzero(ref != ((s - cr) <= TH)))
+        tot += s.size
+    assert tot > 10_000_000 and bad == 0
+
+
+def _round_down(x64):
+    """float32 rounding of float64 values toward -inf."""
+    y = x64.astype(F32)
+    hi = y.astype(np.float64) > x64
+    y[hi] = np.nextafter(y[hi], F32(-np.inf))
+    return y
+
+
+def _round_up(x64):
+    y = x64.astype(F32)
+    lo = y.astype(np.float64) < x64
+    y[lo] = np.nextafter(y[lo], F32(np.inf))
+    return y
+
+
+def _coord_ref(tau):
+    """The reference: gamma in double, stored to float, + 0.5/512 in float."""
+    t = tau.astype(np.float64)
+    g = (t / (1.0 + t)).astype(F32)
+    tc = (g.astype(np.float64) + 0.5 / 512).astype(F32)
+    ok = (tc >= 0) & (tc <= 1)
+    idx = np.minimum((tc * F32(512)).astype(np.uint32), 511)
+    return np.where(ok, idx.astype(np.int64), -1)
+
+
+def _floor512(t):
+    # RD(t * 512 + 2^23) read back as an integer: floor(t * 512) for t in [0, 1]
+    x = t.astype(np.float64) * 512.0 + 8388608.0
+    return _round_down(x).view(np.uint32).astype(np.int64) - 0x4b000000
+
+
+def test_psi_coordinate_bracket():
+    rng = np.random.default_rng(11)
+    tau = np.concatenate([(10.0 ** rng.uniform(-10, 6, 2_000_000)).astype(F32),
+                          rng.uniform(0, 4, 1_000_000).astype(F32)])
+    tau = tau[(tau > 0) & (tau < F32(1048576.0))]
+    ref = _coord_ref(tau)
+    d = (F32(1.0) + tau).astype(F32)
+    q = (tau.astype(np.float64) / d.astype(np.float64)).astype(F32)
+    accepted = 0
+    for k in (-2, -1, 0, 1, 2):  # any estimate within 2 ulp of the float quotient
+        g = q
+        for _ in range(abs(k)):
+            g = np.nextafter(g, F32(np.inf) if k > 0 else F32(-np.inf))
+        tlo = ((_round_down(g.astype(np.float64) - 2.0 ** -20)).astype(np.float64) + 2.0 ** -10).astype(F32)
+        thi = ((_round_up(g.astype(np.float64) + 2.0 ** -20)).astype(np.float64) + 2.0 ** -10).astype(F32)
+        flo, fhi = _floor512(tlo), _floor512(thi)
+        fast = (thi <= 1) & (flo == fhi)
+        assert np.array_equal(np.minimum(flo[fast], 511), ref[fast])
+        out = tlo > 1
+        assert np.all(ref[out & ~fast] == -1)
+        accepted += int(np.count_nonzero(fast | out))
+    # the double division is needed for about one tau in a thousand
+    assert accepted > 0.99 * 5 * tau.size

@@ -146,6 +146,73 @@ __device__ __forceinline__ bool entry_inside(const EntryEdges& E, float ox, floa
   return (cy >= 0.0f) && (cz >= 0.0f) && (fadd(cy, cz) <= E.cx);
 }
 
+// psi-table coordinate of one extinction tau (vfRayKernelCPU.cc:462-471):
+// gamma = tau / (1.0 + tau) in double, stored to float; tc = gamma + 0.5/512;
+// the step ends when tc is outside [0, 1]; the coordinate is (uint)(tc*512).
+// Returns that coordinate (at most 511), or -1 when the step ends.
+//
+// The quotient only selects an integer, so it is first estimated in float:
+// for 0 < tau < 2^20, g = __fdividef(tau, 1 + tau) is within 2^-21.4 of
+// tau / (1 + tau) (2 ulp for the quotient, half an ulp for the float sum),
+// and so is the reference's double quotient (within 2^-52).  The floats
+// lo = RD(g - 2^-20) and hi = RU(g + 2^-20) then bracket the reference's
+// (float)gamma, and tc and the coordinate are non-decreasing in gamma: when
+// lo and hi give the same coordinate (all but about one case in 2^10) it is
+// the reference's.  The other cases take the double division, as written
+// in the reference.  floor(tc * 512) for tc in [0, 1] is read off
+// RD(tc * 512 + 2^23) (tc * 512 is exact), which needs no conversion unit.
+__device__ __forceinline__ int psi_coord(float tau) {
+  if (tau == 0.0f) return 0;  // gamma = 0, tc = 2^-10
+  if (tau > 0.0f && tau < 1048576.0f) {
+    const float g = __fdividef(tau, fadd(1.0f, tau));
+    const float tlo = fadd(__fsub_rd(g, 0x1p-20f), 0x1p-10f);
+    const float thi = fadd(__fadd_ru(g, 0x1p-20f), 0x1p-10f);
+    const float flo = __fmaf_rd(tlo, 512.0f, 0x1p23f);
+    const float fhi = __fmaf_rd(thi, 512.0f, 0x1p23f);
+    if (thi <= 1.0f && flo == fhi) return (int)min(__float_as_uint(flo) - 0x4b000000u, 511u);
+    if (tlo > 1.0f) return -1;
+  }
+  const double t = (double)tau;
+  const float g = (float)ddiv(t, dadd(1.0, t));
+  const float tc = fadd(g, 0.5f / 512.0f);  // one float rounding either way
+  if ((tc < 0.0f) || (tc > 1.0f)) return -1;
+  return (int)min((uint32_t)fmul(tc, 512.0f), 511u);
+}
+
+// zeta = (float)exp(x) for the double x = -(tau_f*0.5 + tau_b*0.5)
+// (vfRayKernelCPU.cc:459).  Table-driven exponential (P. T. P. Tang, "Table-
+// driven implementation of the exponential function in IEEE floating-point
+// arithmetic", ACM TOMS 15(2), 1989): x = (64m + j) ln2/64 + r with
+// |r| <= ln2/128, exp(x) = 2^m * 2^(j/64) * p(r), p the degree-4 Taylor
+// polynomial.  Its relative error is below 2^-44.4 (truncation
+// (ln2/128)^5/120, plus a few roundings), i.e. under 360 units in the last
+// place of the double result, and the reference's double exp is within
+// 0.52 of those units of the true value.  Rounded to float, the estimate
+// then gives the reference's zeta unless the 29 bits that rounding drops
+// lie within 1024 units of the half-way pattern 2^28 (about one case in
+// 2^18): those cases, and x outside [-80, 0], take the double exp.
+// e2tab holds 2^(j/64), j = 0..63, rounded to double.
+__device__ __forceinline__ float zeta_of(double x, const double* e2tab) {
+  if (x >= -80.0 && x <= 0.0) {
+    const double kShift = 0x1.8p52;  // adding 1.5 * 2^52 rounds to an integer
+    const double t = __fma_rn(x, 0x1.71547652b82fep+6 /* 64 / ln2 */, kShift);
+    const int k = __double2loint(t);  // round(x * 64 / ln2), -7400 <= k <= 0
+    const double kd = dsub(t, kShift);
+    double r = __fma_rn(-kd, 0x1.62e42fefa39efp-7, x);   // ln2/64, leading part
+    r = __fma_rn(-kd, 0x1.abc9e3b39803fp-62, r);         // ln2/64, trailing part
+    double p = __fma_rn(r, 1.0 / 24.0, 1.0 / 6.0);
+    p = __fma_rn(p, r, 0.5);
+    p = __fma_rn(p, r, 1.0);
+    p = __fma_rn(p, r, 1.0);
+    double e = dmul(e2tab[k & 63], p);
+    // times 2^(k >> 6): the exponent field stays far above the subnormals
+    e = __hiloint2double(__double2hiint(e) + (k >> 6) * (1 << 20), __double2loint(e));
+    const uint32_t dropped = (uint32_t)__double2loint(e) & 0x1fffffffu;
+    if (dropped - (0x10000000u - 1024u) > 2048u) return (float)e;
+  }
+  return (float)exp(x);
+}
+
 // Orderable encoding of floats for atomicMin/atomicMax on unsigned ints.
 __device__ __forceinline__ uint32_t f2ord(float f) {
   uint32_t b = __float_as_uint(f);

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -363,6 +364,7 @@ int Batch::enqueue_c() {
   P.ent_cap = (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu);
   P.tf = C.d_tf;
   P.psi = C.d_psi;
+  P.e2tab = reinterpret_cast<const double*>(C.d_tf + 256);
   P.step_cap = C.step_cap;
   P.refill = C.tune.refill;
   const int blocks = C.num_sms * C.traverse_blocks_per_sm(mode);
@@ -582,13 +584,19 @@ int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
     vfr_psi_table(gen.data());
     psi = gen.data();
   }
+  // the transfer function (256 float4) is followed by the 64 doubles
+  // 2^(j/64) of the traversal's table-driven exponential
   if (!C.d_tf) {
-    int rc = C.cuda(cudaMalloc(&C.d_tf, sizeof(float4) * 256), "tf alloc");
+    int rc = C.cuda(cudaMalloc(&C.d_tf, sizeof(float4) * 256 + sizeof(double) * 64), "tf alloc");
     if (!rc) rc = C.cuda(cudaMalloc(&C.d_psi, sizeof(float) * 512 * 512), "psi alloc");
     if (rc) return rc;
   }
   cudaStreamSynchronize(C.stream);
+  double e2[64];
+  for (int j = 0; j < 64; ++j) e2[j] = (double)std::exp2l((long double)j / 64.0L);
   int rc = C.cuda(cudaMemcpy(C.d_tf, tf, sizeof(float) * 1024, cudaMemcpyHostToDevice), "tf upload");
+  if (!rc)
+    rc = C.cuda(cudaMemcpy(C.d_tf + 256, e2, sizeof(e2), cudaMemcpyHostToDevice), "exp2 upload");
   if (!rc)
     rc = C.cuda(cudaMemcpy(C.d_psi, psi, sizeof(float) * 512 * 512, cudaMemcpyHostToDevice),
                 "psi upload");

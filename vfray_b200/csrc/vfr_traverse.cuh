@@ -17,8 +17,14 @@
 namespace vfr {
 
 // One exit candidate (vfRayKernelCPU.cc:312-348), branch-free.  The slack
-// test (double)(c1+c2) <= (double)cr + 1e-12 is decided in float unless cr is
-// below 2^-16: for larger cr the next float above cr is more than 1e-12 away.
+// test (double)(c1+c2) <= (double)cr + 1e-12 (:341-342) is decided in float:
+// for a float sum s and cr >= 0x2b8cbccd (faces below RDELTA are skipped) it
+// holds exactly when s - cr rounded to float is at most 0x2b8cbccc, the
+// largest float below 1e-12.  For s <= cr both hold; for cr < s <= 2cr the
+// difference is exact (Sterbenz) and a multiple of ulp(cr) >= 2^-63, and no
+// such multiple lies within the double rounding error of cr + 1e-12 (below
+// 2^(k-28) for multiples of 2^k) of 1e-12, whose distance to the multiples of
+// 2^-63 is 2^-67.8; for s > 2cr the difference exceeds cr > 1e-12.
 __device__ __forceinline__ bool exit_test(const float4& a, const float4& b, const float4& c,
                                           float ox, float oy) {
   const float v1x = fsub(b.x, a.x), v1y = fsub(b.y, a.y);
@@ -33,8 +39,7 @@ __device__ __forceinline__ bool exit_test(const float4& a, const float4& b, cons
   const float c1 = fsub(fmul(w1x, v0y), fmul(w1y, v0x));
   const float c2 = fsub(fmul(v0x, w2y), fmul(v0y, w2x));
   const float sum = fadd(c1, c2);
-  const bool within = (sum <= cr) ||
-                      (cr < 1.52587890625e-05f && (double)sum <= dadd((double)cr, kRDelta));
+  const bool within = fsub(sum, cr) <= __uint_as_float(0x2b8cbcccu);
   return !skip && (c1 >= 0.0f) && (c2 >= 0.0f) && within;
 }
 
@@ -56,7 +61,7 @@ struct Ray {
   const float4* vert;
   uint32_t j, nT, cap;
   float maxEdge;
-  float4 cb;                   // colorBack
+  uint32_t cbi;                // colorBack: its transfer-function entry
   uint32_t t, f, p, iters;
   float ox, oy, zp, sp;
   float ar, ag, ab, tr, lastZ;
@@ -80,7 +85,7 @@ __device__ __forceinline__ void begin_segment(const JobDev& J, const float4* s_t
   R.zp = zp;
   R.sp = sp;
   R.lastZ = zp;
-  R.cb = s_tf[(uint32_t)fmul(255.0f, sp)];
+  R.cbi = (uint32_t)fmul(255.0f, sp);
 }
 
 // Composited mode: the next entry of the pixel in (depth, index) descending
@@ -132,7 +137,8 @@ __device__ __forceinline__ void finish_pixel(const JobDev& J, const Ray& R) {
 enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kAbandon = 2, kCap = 3, kRange = 4 };
 
 // One iteration of the reference's while loop (:302-542).
-__device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* s_tf, Ray& R) {
+__device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* s_tf,
+                                         const double* s_e2, Ray& R) {
   if (++R.iters > R.cap) return kCap;
   const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
@@ -164,28 +170,19 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* 
   dz = below_rdelta(dz) ? 0.0f : dz;
   if ((sn < 0.0f) || (sn > 1.0f)) return kSegmentEnd;  // :446
   dz = (dz == 0.0f) ? 0.0f : fdiv(dz, R.maxEdge);
-  const float4 cf = s_tf[(uint32_t)fmul(255.0f, sn)];
-  const float taux = fmul(cf.w, dz), tauy = fmul(R.cb.w, dz);
+  const uint32_t tfi = (uint32_t)fmul(255.0f, sn);
+  const float4 cf = s_tf[tfi], cb = s_tf[R.cbi];
+  const float taux = fmul(cf.w, dz), tauy = fmul(cb.w, dz);
   {
-    const float zeta = (float)exp(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)));
-    // tau / (1.0 + tau) in double; a zero numerator is taken apart so that
-    // the division never meets its special-case path
-    const double tx1 = taux == 0.0f ? 1.0 : (double)taux;
-    const double ty1 = tauy == 0.0f ? 1.0 : (double)tauy;
-    const float gx = taux == 0.0f ? 0.0f : (float)ddiv(tx1, dadd(1.0, tx1));
-    const float gy = tauy == 0.0f ? 0.0f : (float)ddiv(ty1, dadd(1.0, ty1));
-    // gamma + 0.5/512: a float plus an exactly representable constant,
-    // rounded once to float either way (double rounding of + is innocuous)
-    const float tcx = fadd(gx, 0.5f / 512.0f), tcy = fadd(gy, 0.5f / 512.0f);
-    if ((tcx < 0.0f) || (tcx > 1.0f) || (tcy < 0.0f) || (tcy > 1.0f)) return kSegmentEnd;  // :468
-    const uint32_t pi = min((uint32_t)fmul(tcx, 512.0f), 511u);
-    const uint32_t pj = min((uint32_t)fmul(tcy, 512.0f), 511u);
-    const double psi = (double)__ldg(P.psi + pi * 512u + pj);
+    const float zeta = zeta_of(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)), s_e2);
+    const int ci = psi_coord(taux), cj = psi_coord(tauy);
+    if ((ci | cj) < 0) return kSegmentEnd;  // :468
+    const double psi = (double)__ldg(P.psi + (uint32_t)ci * 512u + (uint32_t)cj);
     const double dzeta = (double)zeta;
     const double ca = dsub(1.0, psi), cbk = dsub(psi, dzeta);
-    const float fr = (float)dadd(dmul((double)cf.x, ca), dmul((double)R.cb.x, cbk));
-    const float fg = (float)dadd(dmul((double)cf.y, ca), dmul((double)R.cb.y, cbk));
-    const float fb = (float)dadd(dmul((double)cf.z, ca), dmul((double)R.cb.z, cbk));
+    const float fr = (float)dadd(dmul((double)cf.x, ca), dmul((double)cb.x, cbk));
+    const float fg = (float)dadd(dmul((double)cf.y, ca), dmul((double)cb.y, cbk));
+    const float fb = (float)dadd(dmul((double)cf.z, ca), dmul((double)cb.z, cbk));
     const float fw = fsub(1.0f, zeta);           // (float)(1.0 - zeta), innocuous double rounding
     const double keep = dsub(1.0, (double)fw);   // exact
     R.ar = (float)dadd((double)fr, dmul(keep, (double)R.ar));
@@ -194,7 +191,7 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* 
     R.tr = fmul(R.tr, zeta);
   }
   R.lastZ = zn;
-  R.cb = cf;
+  R.cbi = tfi;
   if (leaving) return kSegmentEnd;  // :535
   // advance to tn through its face fn: slots fn..fn+2 are the exit face's
   // vertices in tn's order (permutation code), slot fn+3 is the loaded vertex
@@ -244,7 +241,9 @@ __device__ __forceinline__ void flush(const TraverseParams& P, Tally& T) {
 template <int kMode, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParams P) {
   __shared__ float4 s_tf[256];
+  __shared__ double s_e2[64];
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tf[i] = P.tf[i];
+  for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) s_e2[i] = P.e2tab[i];
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt_mask = (1u << lane) - 1u;
@@ -311,7 +310,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
       continue;
     }
     if (!active) continue;
-    const uint32_t res = step(P, s_tf, R);
+    const uint32_t res = step(P, s_tf, s_e2, R);
     if (res == kContinue) continue;
     if (res == kSegmentEnd) {
       if (kMode == 1) {

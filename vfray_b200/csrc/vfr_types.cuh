@@ -54,6 +54,7 @@ struct TraverseParams {
   uint32_t ent_cap;
   const float4* tf;          // 256 RGBA
   const float* psi;          // 512 x 512
+  const double* e2tab;       // 2^(j/64), j = 0..63
   uint32_t step_cap;         // 0: 4 * nT + 64 of each job's mesh
   uint32_t refill;           // refill a warp's idle lanes once this many are idle
 };
