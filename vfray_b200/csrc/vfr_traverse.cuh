@@ -54,6 +54,17 @@ __device__ __forceinline__ uint32_t pick3u(uint32_t i, uint32_t x1, uint32_t x2,
   return i == 1 ? x1 : (i == 2 ? x2 : x3);
 }
 
+// Per-CTA copies of the small tables: the transfer function's alpha in float
+// and its colour promoted to double (the compositing multiplies colours in
+// double, vfRayKernelCPU.cc:473-476, so the promotion is done once here), and
+// 2^(j/64), j = 0..63, for zeta_of.
+struct SharedTables {
+  double2 rg[256];
+  double b[256];
+  float a[256];
+  double e2[64];
+};
+
 struct Ray {
   float4 r0, r1, r2, r3;       // vertices rotated by the entry face
   WalkRec w;                   // walk record of the current tet
@@ -71,8 +82,8 @@ struct Ray {
 };
 
 // Start a segment at external face e with entry depth zp (:256-279).
-__device__ __forceinline__ void begin_segment(const JobDev& J, const float4* s_tf, Ray& R,
-                                              uint32_t e, float zp, float sp) {
+__device__ __forceinline__ void begin_segment(const JobDev& J, Ray& R, uint32_t e, float zp,
+                                              float sp) {
   const uint2 tf = J.extf[e];
   R.t = tf.x;
   R.f = tf.y;
@@ -92,7 +103,7 @@ __device__ __forceinline__ void begin_segment(const JobDev& J, const float4* s_t
 // order after the last one taken, skipping entries above the depth where the
 // previous segment left the mesh.  Returns false when the list is done.
 __device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev& J,
-                                           const float4* s_tf, Ray& R, bool first) {
+                                           Ray& R, bool first) {
   for (;;) {
     float bz = -INFINITY;
     uint32_t be = 0, bzb = 0;
@@ -116,7 +127,7 @@ __device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev
     first = false;
     if (bz > R.exitZ) continue;  // behind the ray already
     const float4 p0 = J.planes[2 * (size_t)be], p1 = J.planes[2 * (size_t)be + 1];
-    begin_segment(J, s_tf, R, be, bz, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
+    begin_segment(J, R, be, bz, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
     return true;
   }
 }
@@ -137,8 +148,7 @@ __device__ __forceinline__ void finish_pixel(const JobDev& J, const Ray& R) {
 enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kAbandon = 2, kCap = 3, kRange = 4 };
 
 // One iteration of the reference's while loop (:302-542).
-__device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* s_tf,
-                                         const double* s_e2, Ray& R) {
+__device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTables& S, Ray& R) {
   if (++R.iters > R.cap) return kCap;
   const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
@@ -170,19 +180,20 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const float4* 
   dz = below_rdelta(dz) ? 0.0f : dz;
   if ((sn < 0.0f) || (sn > 1.0f)) return kSegmentEnd;  // :446
   dz = (dz == 0.0f) ? 0.0f : fdiv(dz, R.maxEdge);
-  const uint32_t tfi = (uint32_t)fmul(255.0f, sn);
-  const float4 cf = s_tf[tfi], cb = s_tf[R.cbi];
-  const float taux = fmul(cf.w, dz), tauy = fmul(cb.w, dz);
+  const uint32_t tfi = (uint32_t)fmul(255.0f, sn);  // colorFront (:452)
+  const float taux = fmul(S.a[tfi], dz), tauy = fmul(S.a[R.cbi], dz);
   {
-    const float zeta = zeta_of(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)), s_e2);
+    const float zeta = zeta_of(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)), S.e2);
     const int ci = psi_coord(taux), cj = psi_coord(tauy);
     if ((ci | cj) < 0) return kSegmentEnd;  // :468
     const double psi = (double)__ldg(P.psi + (uint32_t)ci * 512u + (uint32_t)cj);
     const double dzeta = (double)zeta;
     const double ca = dsub(1.0, psi), cbk = dsub(psi, dzeta);
-    const float fr = (float)dadd(dmul((double)cf.x, ca), dmul((double)cb.x, cbk));
-    const float fg = (float)dadd(dmul((double)cf.y, ca), dmul((double)cb.y, cbk));
-    const float fb = (float)dadd(dmul((double)cf.z, ca), dmul((double)cb.z, cbk));
+    const double2 frg = S.rg[tfi], brg = S.rg[R.cbi];
+    const double fbl = S.b[tfi], bbl = S.b[R.cbi];
+    const float fr = (float)dadd(dmul(frg.x, ca), dmul(brg.x, cbk));
+    const float fg = (float)dadd(dmul(frg.y, ca), dmul(brg.y, cbk));
+    const float fb = (float)dadd(dmul(fbl, ca), dmul(bbl, cbk));
     const float fw = fsub(1.0f, zeta);           // (float)(1.0 - zeta), innocuous double rounding
     const double keep = dsub(1.0, (double)fw);   // exact
     R.ar = (float)dadd((double)fr, dmul(keep, (double)R.ar));
@@ -240,10 +251,14 @@ __device__ __forceinline__ void flush(const TraverseParams& P, Tally& T) {
 // (2: no spills; 3: 80 registers, a few spilled to L1).
 template <int kMode, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParams P) {
-  __shared__ float4 s_tf[256];
-  __shared__ double s_e2[64];
-  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tf[i] = P.tf[i];
-  for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) s_e2[i] = P.e2tab[i];
+  __shared__ SharedTables S;
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+    const float4 c = P.tf[i];
+    S.rg[i] = make_double2((double)c.x, (double)c.y);
+    S.b[i] = (double)c.z;
+    S.a[i] = c.w;
+  }
+  for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) S.e2[i] = P.e2tab[i];
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt_mask = (1u << lane) - 1u;
@@ -285,7 +300,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
           if (kMode == 0) {
             const uint32_t e = (uint32_t)J.winner[R.p];
             const float4 p0 = J.planes[2 * (size_t)e], p1 = J.planes[2 * (size_t)e + 1];
-            begin_segment(J, s_tf, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
+            begin_segment(J, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
                           plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
             active = true;
           } else {
@@ -298,7 +313,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
             if (b1 > P.ent_cap) {
               T.status |= 16u;  // VFR_DEV_OVERFLOW: the caller renders again with room
             } else {
-              active = next_entry(P, J, s_tf, R, true);
+              active = next_entry(P, J, R, true);
               if (!active) finish_pixel(J, R);
             }
           }
@@ -310,12 +325,12 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
       continue;
     }
     if (!active) continue;
-    const uint32_t res = step(P, s_tf, s_e2, R);
+    const uint32_t res = step(P, S, R);
     if (res == kContinue) continue;
     if (res == kSegmentEnd) {
       if (kMode == 1) {
         R.exitZ = R.lastZ;
-        if (next_entry(P, P.jobs[R.j], s_tf, R, false)) continue;
+        if (next_entry(P, P.jobs[R.j], R, false)) continue;
       }
       finish_pixel(P.jobs[R.j], R);
     } else if (res == kAbandon) {
