@@ -81,18 +81,28 @@ struct Ray {
   float exitZ;
 };
 
+// Read-only loads of the mesh through the non-coherent path (the arrays are
+// not written while the traversal runs).
+__device__ __forceinline__ WalkRec ldg_walk(const WalkRec* w, uint32_t t) {
+  const uint4* p = reinterpret_cast<const uint4*>(w + t);
+  WalkRec r;
+  r.n = __ldg(p);
+  r.q = __ldg(p + 1);
+  return r;
+}
+
 // Start a segment at external face e with entry depth zp (:256-279).
 __device__ __forceinline__ void begin_segment(const JobDev& J, Ray& R, uint32_t e, float zp,
                                               float sp) {
-  const uint2 tf = J.extf[e];
+  const uint2 tf = __ldg(J.extf + e);
   R.t = tf.x;
   R.f = tf.y;
-  const uint4 id = J.tet[R.t];
-  R.w = R.walk[R.t];
-  R.r0 = R.vert[sel4(id, R.f)];
-  R.r1 = R.vert[sel4(id, (R.f + 1) & 3u)];
-  R.r2 = R.vert[sel4(id, (R.f + 2) & 3u)];
-  R.r3 = R.vert[sel4(id, (R.f + 3) & 3u)];
+  const uint4 id = __ldg(J.tet + R.t);
+  R.w = ldg_walk(R.walk, R.t);
+  R.r0 = __ldg(R.vert + sel4(id, R.f));
+  R.r1 = __ldg(R.vert + sel4(id, (R.f + 1) & 3u));
+  R.r2 = __ldg(R.vert + sel4(id, (R.f + 2) & 3u));
+  R.r3 = __ldg(R.vert + sel4(id, (R.f + 3) & 3u));
   R.zp = zp;
   R.sp = sp;
   R.lastZ = zp;
@@ -164,8 +174,8 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   WalkRec N = R.w;
   float4 nv = R.r0;
   if (!leaving) {
-    N = R.walk[tn];
-    nv = R.vert[q & 0x07ffffffu];
+    N = ldg_walk(R.walk, tn);
+    nv = __ldg(R.vert + (q & 0x07ffffffu));
   }
   // exit face (ex, ex+1, ex+2) = (r_i, r_i+1, r_i+2)
   const float4 a = pick3(i, R.r1, R.r2, R.r3);
@@ -215,11 +225,11 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
     R.r2 = m2 == 0 ? a : (m2 == 1 ? b : c);
     R.r3 = nv;
   } else {  // shared face not matched by vertex ids: reload the tet's vertices
-    const uint4 id = P.jobs[R.j].tet[tn];
-    R.r0 = R.vert[sel4(id, fn)];
-    R.r1 = R.vert[sel4(id, (fn + 1) & 3u)];
-    R.r2 = R.vert[sel4(id, (fn + 2) & 3u)];
-    R.r3 = R.vert[sel4(id, (fn + 3) & 3u)];
+    const uint4 id = __ldg(P.jobs[R.j].tet + tn);
+    R.r0 = __ldg(R.vert + sel4(id, fn));
+    R.r1 = __ldg(R.vert + sel4(id, (fn + 1) & 3u));
+    R.r2 = __ldg(R.vert + sel4(id, (fn + 2) & 3u));
+    R.r3 = __ldg(R.vert + sel4(id, (fn + 3) & 3u));
   }
   R.w = N;
   R.t = tn;
@@ -325,7 +335,9 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
       continue;
     }
     if (!active) continue;
-    const uint32_t res = step(P, S, R);
+    // two steps per pass of the loop: the refill test runs half as often
+    uint32_t res = step(P, S, R);
+    if (res == kContinue) res = step(P, S, R);
     if (res == kContinue) continue;
     if (res == kSegmentEnd) {
       if (kMode == 1) {
