@@ -65,7 +65,8 @@ class Oracle:
             build(reference=False)
         self.lib = C.CDLL(path)
         L = self.lib
-        for name in ("vo_render_ref", "vo_winners", "vo_trace_pixels", "vo_render_composited"):
+        for name in ("vo_render_ref", "vo_winners", "vo_trace_pixels", "vo_render_composited",
+                     "vo_render_ref_fp64"):
             getattr(L, name).restype = C.c_int
         L.vo_compact.restype = C.c_uint32
 
@@ -112,6 +113,16 @@ class Oracle:
             raise ValueError("oracle rejected the mesh")
         return dict(rgb8=rgb, rgba=rgba, writer=wr, steps=st, face_comp=fc[:n],
                     face_abandon=fa[:n], nvis=n)
+
+    def render_ref_fp64(self, m, W, H):
+        """FP64 rerun of render_ref along the same traversal: (H, W, 4)
+        float64 clamped colour + alpha of each pixel's writing ray."""
+        out = np.zeros((H, W, 4), np.float64)
+        n = self.lib.vo_render_ref_fp64(C.byref(m), C.c_uint32(W), C.c_uint32(H),
+                                        out.ctypes.data_as(C.c_void_p))
+        if n < 0:
+            raise ValueError("oracle rejected the mesh")
+        return out
 
     def winners(self, m, W, H):
         wr = np.zeros((H, W), np.int32)

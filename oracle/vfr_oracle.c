@@ -161,12 +161,85 @@ typedef struct {
   float lastZ;
 } ray_state;
 
+/* FP64 rerun of a ray: the tet sequence and every decision come from the
+ * float traversal; along that same path the colour is recomputed entirely
+ * in double (planes, depths, tau, zeta, gamma and the psi index, the sum),
+ * from the double pixel coordinate.  The tables (TF, psi) are the same. */
+typedef struct {
+  double ox, oy, acc[3], trans, zp, cb[4];
+} ray64;
+
+typedef struct { double zx, zy, zz, sx, sy, sz; } face64;
+
+static void plane64(f4 a, f4 b, f4 c, face64* f) {
+  double c0x = a.x, c0y = b.x, c0z = c.x, c1x = a.y, c1y = b.y, c1z = c.y;
+  double det = c0x * (c1y - c1z) - c1x * (c0y - c0z) + (c0y * c1z - c1y * c0z);
+  if (fabs(det) < RDELTA) det = RDELTA;
+  double t[2][3] = {{a.z, b.z, c.z}, {a.w, b.w, c.w}};
+  double o[2][3];
+  for (int k = 0; k < 2; ++k) {
+    double tx = t[k][0], ty = t[k][1], tz = t[k][2];
+    double mx = ty - tz, my = ty * c1z - c1y * tz, mz = c0y * tz - ty * c0z;
+    o[k][0] = (tx * (c1y - c1z) - c1x * mx + my) / det;
+    o[k][1] = (c0x * mx - tx * (c0y - c0z) + mz) / det;
+    o[k][2] = (c0x * (-my) - c1x * mz + tx * (c0y * c1z - c1y * c0z)) / det;
+  }
+  f->zx = o[0][0]; f->zy = o[0][1]; f->zz = o[0][2];
+  f->sx = o[1][0]; f->sy = o[1][1]; f->sz = o[1][2];
+}
+
+static void tf64(const vo_mesh* m, double s, double* c) {
+  if (!(s >= 0.0)) s = 0.0;
+  if (s > 1.0) s = 1.0;
+  uint32_t i = (uint32_t)(255.0 * s);
+  if (i > 255) i = 255;
+  for (int k = 0; k < 4; ++k) c[k] = m->tf[4 * i + k];
+}
+
+static uint32_t psi_index64(double tau) {
+  double tc = tau / (1.0 + tau) + 0.5 / 512;
+  if (!(tc >= 0.0)) tc = 0.0;
+  uint32_t i = (uint32_t)(tc * 512);
+  return i > 511 ? 511 : i;
+}
+
+static void ray64_begin(const vo_mesh* m, uint32_t t, uint32_t f, ray64* D) {
+  f4 v0 = vget(m, m->tet[4 * (size_t)t + f]);
+  f4 v1 = vget(m, m->tet[4 * (size_t)t + ((f + 1) & 3)]);
+  f4 v2 = vget(m, m->tet[4 * (size_t)t + ((f + 2) & 3)]);
+  face64 F;
+  plane64(v0, v1, v2, &F);
+  D->zp = D->ox * F.zx + D->oy * F.zy + F.zz;
+  tf64(m, D->ox * F.sx + D->oy * F.sy + F.sz, D->cb);
+}
+
+static void ray64_step(const vo_mesh* m, f4 a, f4 b, f4 c, ray64* D) {
+  face64 F;
+  plane64(a, b, c, &F);
+  double zn = D->ox * F.zx + D->oy * F.zy + F.zz;
+  double sn = D->ox * F.sx + D->oy * F.sy + F.sz;
+  double dz = fabs(D->zp - zn);
+  if (dz < RDELTA) dz = 0.0;
+  dz /= m->maxEdge;
+  double cf[4];
+  tf64(m, sn, cf);
+  double tf = cf[3] * dz, tb = D->cb[3] * dz;
+  double zeta = exp(-(tf * 0.5 + tb * 0.5));
+  double psi = m->psi[psi_index64(tf) * 512 + psi_index64(tb)];
+  for (int k = 0; k < 3; ++k)
+    D->acc[k] = cf[k] * (1.0 - psi) + D->cb[k] * (psi - zeta) + zeta * D->acc[k];
+  D->trans *= zeta;
+  for (int k = 0; k < 4; ++k) D->cb[k] = cf[k];
+  D->zp = zn;
+}
+
 /* One ray segment from entry (t, f) with entry depth/scalar (zp, sp),
  * :276-542.  Returns 0, or -1 on the :365 `return` (adjacency that does
  * not point back). */
 static int trace(const vo_mesh* m, float ox, float oy, uint32_t t, uint32_t f, float zpx,
-                 float zpy, ray_state* R) {
+                 float zpy, ray_state* R, ray64* D) {
   f4 cb = tfget(m, zpy);
+  if (D) ray64_begin(m, t, f, D);
   uint32_t tpx = t, tpy = f;
   R->lastZ = zpx;
   for (;;) {
@@ -234,6 +307,7 @@ static int trace(const vo_mesh* m, float ox, float oy, uint32_t t, uint32_t f, f
     R->trans = R->trans * zeta;
     R->comps++;
     R->lastZ = znx;
+    if (D) ray64_step(m, fv[(tny + 0) & 3], fv[(tny + 1) & 3], fv[(tny + 2) & 3], D);
     cb = cf;
     if (tnx == tpx) break; /* :535 left the mesh */
     tpx = tnx;
@@ -267,8 +341,9 @@ static int prepare(const vo_mesh* m, uint32_t W, uint32_t H, uint32_t** visExt,
 
 static inline int in_image(uint32_t x, uint32_t y, uint32_t W, uint32_t H) { return x < W && y < H; }
 
-int vo_render_ref(const vo_mesh* m, uint32_t W, uint32_t H, uint8_t* rgb8, float* rgba,
-                  int32_t* writer, uint32_t* steps, uint64_t* faceComp, uint8_t* faceAbandon) {
+static int render_ref(const vo_mesh* m, uint32_t W, uint32_t H, uint8_t* rgb8, float* rgba,
+                      int32_t* writer, uint32_t* steps, uint64_t* faceComp,
+                      uint8_t* faceAbandon, double* rgba64) {
   uint32_t *vis, *bb;
   vo_face* faces;
   int nv = prepare(m, W, H, &vis, &bb, &faces);
@@ -278,6 +353,7 @@ int vo_render_ref(const vo_mesh* m, uint32_t W, uint32_t H, uint8_t* rgb8, float
   if (rgba) memset(rgba, 0, np * 4 * sizeof(float));
   if (writer) for (size_t p = 0; p < np; ++p) writer[p] = -1;
   if (steps) memset(steps, 0, np * sizeof(uint32_t));
+  if (rgba64) memset(rgba64, 0, np * 4 * sizeof(double));
   for (int i = 0; i < nv; ++i) {
     uint32_t e = vis[i];
     entry_face E;
@@ -294,7 +370,9 @@ int vo_render_ref(const vo_mesh* m, uint32_t W, uint32_t H, uint8_t* rgb8, float
         float zpy = ox * E.F.sx + oy * E.F.sy + E.F.sz;
         if ((zpy < 0.0) || (zpy > 1.0)) break; /* :274 rest of the column */
         ray_state R = {{0, 0, 0}, 1.0f, 0, 0, 0};
-        int rc = trace(m, ox, oy, E.t, E.f, zpx, zpy, &R);
+        ray64 D = {px * 2.0 / (W - 1.0) - 1.0, py * 2.0 / (H - 1.0) - 1.0, {0, 0, 0}, 1.0, 0,
+                   {0, 0, 0, 0}};
+        int rc = trace(m, ox, oy, E.t, E.f, zpx, zpy, &R, rgba64 ? &D : NULL);
         comps += R.comps;
         if (rc < 0) { abandoned = 1; break; } /* :365 rest of the face */
         if (!in_image(px, py, W, H)) continue;
@@ -302,6 +380,10 @@ int vo_render_ref(const vo_mesh* m, uint32_t W, uint32_t H, uint8_t* rgb8, float
         finalize(&R, rgb8 ? rgb8 + 3 * p : NULL, rgba ? rgba + 4 * p : NULL);
         if (writer) writer[p] = (int32_t)e;
         if (steps) steps[p] = R.iters;
+        if (rgba64) {
+          for (int k = 0; k < 3; ++k) rgba64[4 * p + k] = D.acc[k] > 1.0 ? 1.0 : D.acc[k];
+          rgba64[4 * p + 3] = 1.0 - D.trans;
+        }
       }
     }
     if (faceComp) faceComp[i] = comps;
@@ -309,6 +391,15 @@ int vo_render_ref(const vo_mesh* m, uint32_t W, uint32_t H, uint8_t* rgb8, float
   }
   free(vis); free(bb); free(faces);
   return nv;
+}
+
+int vo_render_ref(const vo_mesh* m, uint32_t W, uint32_t H, uint8_t* rgb8, float* rgba,
+                  int32_t* writer, uint32_t* steps, uint64_t* faceComp, uint8_t* faceAbandon) {
+  return render_ref(m, W, H, rgb8, rgba, writer, steps, faceComp, faceAbandon, NULL);
+}
+
+int vo_render_ref_fp64(const vo_mesh* m, uint32_t W, uint32_t H, double* rgba64) {
+  return render_ref(m, W, H, NULL, NULL, NULL, NULL, NULL, NULL, rgba64);
 }
 
 int vo_winners(const vo_mesh* m, uint32_t W, uint32_t H, int32_t* writer) {
@@ -396,7 +487,7 @@ static void trace_range(void* c_, size_t lo, size_t hi) {
     float zpx = ox * E.F.zx + oy * E.F.zy + E.F.zz;
     float zpy = ox * E.F.sx + oy * E.F.sy + E.F.sz;
     ray_state R = {{0, 0, 0}, 1.0f, 0, 0, 0};
-    if (trace(c->m, ox, oy, E.t, E.f, zpx, zpy, &R) < 0) __atomic_store_n(&c->err, 1, __ATOMIC_RELAXED);
+    if (trace(c->m, ox, oy, E.t, E.f, zpx, zpy, &R, NULL) < 0) __atomic_store_n(&c->err, 1, __ATOMIC_RELAXED);
     finalize(&R, c->rgb8 ? c->rgb8 + 3 * k : NULL, c->rgba ? c->rgba + 4 * k : NULL);
     if (c->steps) c->steps[k] = R.iters;
   }
@@ -453,7 +544,7 @@ static void comp_range(void* c_, size_t lo, size_t hi) {
     for (size_t i = 0; i < n; ++i) {
       if (L[i].z > exitZ) continue;
       uint32_t e = L[i].e;
-      if (trace(c->m, ox, oy, c->m->extf[2 * e], c->m->extf[2 * e + 1], L[i].z, L[i].s, &R) < 0)
+      if (trace(c->m, ox, oy, c->m->extf[2 * e], c->m->extf[2 * e + 1], L[i].z, L[i].s, &R, NULL) < 0)
         __atomic_store_n(&c->err, 1, __ATOMIC_RELAXED);
       exitZ = R.lastZ;
       ++segs;

@@ -55,6 +55,14 @@ int vo_render_ref(const vo_mesh* m, uint32_t W, uint32_t H, uint8_t* rgb8,
                   float* rgba, int32_t* writer, uint32_t* steps,
                   uint64_t* faceComp, uint8_t* faceAbandon);
 
+/* FP64 rerun of vo_render_ref: the same faces, pixels, tet sequences and
+ * decisions (all taken by the float traversal), with each ray's colour
+ * recomputed in double along its path from the double pixel coordinate
+ * (double planes, depths, tau, zeta, gamma, psi index and sum).  rgba64
+ * W*H*4: clamped colour and 1 - prod(zeta) of the writing ray, 0 elsewhere.
+ * Returns as vo_render_ref. */
+int vo_render_ref_fp64(const vo_mesh* m, uint32_t W, uint32_t H, double* rgba64);
+
 /* Per-pixel winner under the reference semantics for a mesh whose adjacency
  * is consistent: the last visible face (highest ext index) that writes the
  * pixel, honouring the column break.  writer W*H, -1 for none. */
