@@ -117,6 +117,25 @@ def make_workload(name, views=64):
     return wl
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise max over ranks of per-rank timings (ms); every rank takes
+    part.  Without a process group, the values themselves."""
+    if not dist:
+        return np.asarray(values, np.float64)
+    import torch
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.cpu().numpy()
+
+
+def whole_job_mrays(rays_per_replica_step, world, steps, ms):
+    """Whole-job throughput: every replica renders the same workload (weak
+    scaling), so the job's rays are world x the replica's, over the slowest
+    rank's time."""
+    return rays_per_replica_step * world * steps / (ms * 1e-3) / 1e6
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -307,18 +326,12 @@ def run_ours(args, rank, world, dist):
         e2e_step()
     t_e2e = (time.perf_counter() - t0) * 1e3
 
-    times = np.array([t_main, t_e2e, t_plain, t_batch], dtype=np.float64)
-    if dist:
-        import torch.distributed as td
-
-        tt = torch.tensor(times, device=dev)
-        td.all_reduce(tt, op=td.ReduceOp.MAX)
-        times = tt.cpu().numpy()
+    times = max_over_ranks([t_main, t_e2e, t_plain, t_batch], dist, dev)
     t_main, t_e2e, t_plain, t_batch = times
     K = args.steps
 
     def mrays(t, k):
-        return rays_step * world * k / (t * 1e-3) / 1e6
+        return whole_job_mrays(rays_step, world, k, t)
 
     value, e2e = mrays(t_main, K), mrays(t_e2e, K)
 
