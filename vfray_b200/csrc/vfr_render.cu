@@ -76,7 +76,10 @@ int Ctx::grow(Buf& b, size_t bytes, const char* what) {
   }
   b.p = nullptr;
   b.cap = 0;
-  const size_t want = bytes + bytes / 8 + 256;
+  // half again as much as asked: a buffer that keeps growing (a server's
+  // batches of varying size) settles after a few steps, and every growth
+  // waits for the device
+  const size_t want = bytes + bytes / 2 + 256;
   int rc = cuda(cudaMalloc(&b.p, want), what);
   if (rc) return rc;
   b.cap = want;

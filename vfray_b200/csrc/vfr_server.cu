@@ -61,6 +61,7 @@ struct Slot {
 struct vfr_server {
   vfr_ctx* ctx = nullptr;
   uint64_t budget = 0, used = 0;
+  size_t copy_threads = std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2));
   uint32_t max_batch = 256;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -114,8 +115,9 @@ int vfr_server::launch(Slot& s, std::vector<Req*>& reqs) {
     if (s.pin) cudaFreeHost(s.pin);
     s.pin = nullptr;
     s.pin_cap = 0;
-    if (cudaMallocHost(&s.pin, pix * 3) != cudaSuccess) rc = VFR_ERR_NOMEM;
-    else s.pin_cap = pix * 3;
+    const size_t want = pix * 3 + pix * 3 / 2;  // headroom: pinning is slow
+    if (cudaMallocHost(&s.pin, want) != cudaSuccess) rc = VFR_ERR_NOMEM;
+    else s.pin_cap = want;
   }
   if (!rc)
     rc = C.cuda(cudaMemcpyAsync(s.pin, s.b.out_rgb8.p, pix * 3, cudaMemcpyDeviceToHost, s.stream),
@@ -139,21 +141,54 @@ void vfr_server::retire(Slot& s) {
   cudaEventSynchronize(s.done);
   std::vector<vfr::ViewCounters> k;
   int rc = s.b.counters(k);
+  // images from the pinned staging into the requests' buffers, split over
+  // a few threads when there is much to copy (the callers' buffers are often
+  // fresh memory whose first touch costs more than the copy)
+  {
+    std::vector<std::pair<size_t, size_t>> span(s.reqs.size());  // (pixel offset, pixels)
+    size_t off = 0, total = 0;
+    for (size_t i = 0; i < s.reqs.size(); ++i) {
+      const size_t np = (size_t)s.reqs[i]->r.W * s.reqs[i]->r.H;
+      span[i] = {off, np};
+      off += np;
+      if (!rc && s.reqs[i]->status == VFR_OK && s.reqs[i]->r.rgb8_host) total += np * 3;
+    }
+    auto copy = [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; ++i) {
+        Req* q = s.reqs[i];
+        if (!rc && q->status == VFR_OK && q->r.rgb8_host)
+          std::memcpy(q->r.rgb8_host, s.pin + 3 * span[i].first, span[i].second * 3);
+      }
+    };
+    const size_t nthreads = std::min<size_t>(copy_threads, std::max<size_t>(1, total >> 23));
+    if (nthreads <= 1) {
+      copy(0, s.reqs.size());
+    } else {  // split by bytes
+      std::vector<std::thread> th;
+      size_t lo = 0, acc = 0, next = 1;
+      for (size_t i = 0; i < s.reqs.size(); ++i) {
+        acc += span[i].second * 3;
+        if (acc >= total * next / nthreads && next < nthreads) {
+          th.emplace_back(copy, lo, i + 1);
+          lo = i + 1;
+          ++next;
+        }
+      }
+      copy(lo, s.reqs.size());
+      for (auto& t : th) t.join();
+    }
+  }
   const Clock::time_point now = Clock::now();
-  size_t off = 0;
   std::lock_guard<std::mutex> g(mu);
   for (size_t i = 0; i < s.reqs.size(); ++i) {
     Req* q = s.reqs[i];
-    const size_t np = (size_t)q->r.W * q->r.H;
     if (q->status == VFR_OK && !rc) {
-      if (q->r.rgb8_host) std::memcpy(q->r.rgb8_host, s.pin + 3 * off, np * 3);
       q->num_rays = k[i].nrays;
       q->num_steps = k[i].steps;
       if (k[i].status) q->status = C.check_status(k[i].status, 0);
     } else if (q->status == VFR_OK) {
       q->status = rc;
     }
-    off += np;
     q->t_done = now;
     q->done = true;
     used -= q->footprint;
