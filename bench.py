@@ -1,7 +1,7 @@
 """Benchmark of the VF-Ray render path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--form batched|plain] [--workload orbit64|mixed|served|convex24]
+                    [--form batched|plain] [--workload orbit64|mixed|served|convex24|large]
 
 Workloads (seeded synthetic meshes, transfer function and cameras):
   orbit64  (default) the carved 64^3 Freudenthal mesh (1,572,864 tets before
@@ -14,6 +14,9 @@ Workloads (seeded synthetic meshes, transfer function and cameras):
            several rates, requests at {256^2, 512^2, 1024^2}; p50/p99 latency
            and Mrays/s per rate.
   convex24 one 512x512 view of the convex 24^3 mesh.
+  large    one 2048x2048 view of the carved 256^3 mesh (100.7 M tets before
+           carving, 85.6 M after: 4.1 GB of tet and walk records, far beyond
+           L2); building the mesh on the host takes about two minutes.
 
 Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events
 on the render stream after an L2 flush (a 256 MiB write) that is not timed;
@@ -54,7 +57,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="batched", choices=["batched", "plain"])
     ap.add_argument("--workload", default="orbit64",
-                    choices=["orbit64", "mixed", "served", "convex24"])
+                    choices=["orbit64", "mixed", "served", "convex24", "large"])
     ap.add_argument("--views", type=int, default=64, help="orbit views (orbit64)")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
@@ -92,6 +95,13 @@ def make_workload(name, views=64):
         wl["meshes"] = [_mesh(64, True)]
         wl["jobs"] = [(0, mv, 512, 512) for mv in synth.orbit_views(views, seed=3)]
         wl["desc"] = f"{views} orbit views at 512x512 of the carved 64^3 Freudenthal mesh"
+    elif name == "large":
+        vert, tet = synth.make_mesh(256, carved=True, view_seed=3)
+        p = vb.prepare(vert, tet)
+        p["n"] = 256
+        wl["meshes"] = [p]
+        wl["jobs"] = [(0, None, 2048, 2048)]
+        wl["desc"] = "one 2048x2048 view of the carved 256^3 Freudenthal mesh (seeded rotation)"
     elif name == "convex24":
         vert, tet = synth.make_mesh(24, carved=False, view_seed=3)
         p = vb.prepare(vert, tet)

@@ -314,6 +314,19 @@ VFR_API int vfr_write_ppm(const char* path, const uint8_t* rgb8, uint32_t W, uin
 /* Parse a psiGammaTable512.h-style C source ("float name[512][512] = {...}"). */
 VFR_API int vfr_read_psi_source(const char* path, float* out512x512);
 
+/* Binary mesh cache (no counterpart in the reference, which re-parses its
+ * text files on every run, vfRay.cu:745-842): the normalised vertices, tets,
+ * conTet, external faces and limits in one file, read back with a few
+ * fread calls.  Reading is two-step like the text readers (NULL buffers:
+ * sizes only); a file whose length does not match its header is refused
+ * with VFR_ERR_IO. */
+VFR_API int vfr_write_mesh_cache(const char* path, const float* vert4, uint32_t nV,
+                                 const uint32_t* tet4, const uint32_t* con4, uint32_t nT,
+                                 const uint32_t* extf2, uint32_t nExt, const float* lmt3);
+VFR_API int vfr_read_mesh_cache(const char* path, float* vert4, uint32_t* nV, uint32_t* tet4,
+                                uint32_t* con4, uint32_t* nT, uint32_t* extf2, uint32_t* nExt,
+                                float* lmt3);
+
 #ifdef __cplusplus
 }
 #endif

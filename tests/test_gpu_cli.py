@@ -59,6 +59,26 @@ def test_cli_renders_like_the_oracle(tmp_path, oracle_lib):
     assert (img.sum(-1) > 0).sum() > 1000
 
 
+def test_cli_binary_cache(tmp_path):
+    """--cache writes <volume>.vfrb after the text files and reads it on the
+    next run; both runs give the same image."""
+    if not os.path.exists(CLI):
+        pytest.skip("driver not built")
+    ds = tmp_path / "tet_offs"
+    ds.mkdir()
+    vert, tet = synth.make_mesh(8, carved=True, view_seed=3)
+    vb.write_off(str(ds / "blob.off"), vert, tet)
+    imgs = []
+    for run in range(2):
+        out = subprocess.run([CLI, "--cache", "--dir", str(ds), "--out", f"r{run}.ppm", "blob"],
+                             cwd=tmp_path, capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stdout + out.stderr
+        assert ("Writing" if run == 0 else "Reading") in out.stdout and "binary cache" in out.stdout
+        imgs.append(read_ppm(tmp_path / f"r{run}.ppm"))
+    assert (ds / "blob.vfrb").exists()
+    assert np.array_equal(imgs[0], imgs[1]) and (imgs[0].sum(-1) > 0).sum() > 1000
+
+
 def test_cli_usage_and_missing_file(tmp_path):
     if not os.path.exists(CLI):
         pytest.skip("driver not built")

@@ -141,3 +141,42 @@ def test_golden_inputs_reproduce(name):
     bytes the reference's precomputation gave."""
     d = load_golden(name)
     assert d["extf"].shape[0] == d["n_ext"]
+
+
+def test_mesh_cache_roundtrip_and_errors(tmp_path):
+    vert, tet = synth.make_mesh(6, carved=True, view_seed=2)
+    p = vb.prepare(vert, tet)
+    path = str(tmp_path / "m.vfrb")
+    vb.write_mesh_cache(path, p)
+    q = vb.read_mesh_cache(path)
+    for k in ("vert", "tet", "con", "extf", "lmt"):
+        assert np.array_equal(p[k], q[k]), k
+    data = open(path, "rb").read()
+    (tmp_path / "short.vfrb").write_bytes(data[:-8])          # truncated
+    (tmp_path / "magic.vfrb").write_bytes(b"X" + data[1:])     # not a cache
+    for bad in ("short.vfrb", "magic.vfrb", "missing.vfrb"):
+        with pytest.raises(vb.VfrError):
+            vb.read_mesh_cache(str(tmp_path / bad))
+
+
+def test_large_off_parsed_in_parallel_like_a_sequential_read(tmp_path):
+    """A file above the parallel threshold (64 MB), written with irregular
+    whitespace (tabs, CRLF, several numbers per line, records split over
+    lines) and trailing text, reads to the same arrays as the numbers it
+    holds, as a sequential operator>> read would."""
+    rng = np.random.default_rng(3)
+    nv, nt = 1_200_000, 2_600_000
+    v = rng.uniform(-1, 1, (nv, 4)).astype(np.float32)
+    t = rng.integers(0, nv, (nt, 4), dtype=np.uint64).astype(np.uint32)
+    toks = np.concatenate([np.char.mod("%.9g", v.ravel().astype(np.float64)),
+                           t.ravel().astype(str)])
+    seps = np.array([" ", "\t", "\n", "\r\n", "  "])[rng.integers(0, 5, toks.size)]
+    body = "".join(np.char.add(toks, seps).tolist())
+    text = f"{nv} {nt}\n" + body + "\ntrailing words 1 2 3\n"
+    assert len(text) > (64 << 20)
+    (tmp_path / "big.off").write_text(text)
+    v2, t2 = vb.read_off(str(tmp_path / "big.off"))
+    assert np.array_equal(v2, v) and np.array_equal(t2, t)
+    (tmp_path / "cut.off").write_text(text[: len(text) // 2])  # too few numbers
+    with pytest.raises(vb.VfrError):
+        vb.read_off(str(tmp_path / "cut.off"))

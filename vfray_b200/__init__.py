@@ -26,6 +26,7 @@ __all__ = [
     "normalize", "rotate", "build_con", "build_extf", "build_lmt", "psi_table", "default_tf",
     "prepare", "read_off", "read_con", "read_extf", "read_lmt", "read_tf", "write_off",
     "write_con", "write_extf", "write_lmt", "write_tf", "write_ppm", "read_psi_source",
+    "write_mesh_cache", "read_mesh_cache",
 ]
 
 
@@ -163,6 +164,31 @@ def read_psi_source(path):
     out = np.empty((512, 512), np.float32)
     check(load().vfr_read_psi_source(path.encode(), ptr(out)), what=path)
     return out
+
+
+def write_mesh_cache(path, p):
+    """Write a prepared mesh (dict of vert, tet, con, extf, lmt as from
+    ``prepare``) to the binary cache."""
+    v, t, c = _f32(p["vert"], (-1, 4)), _u32(p["tet"], (-1, 4)), _u32(p["con"], (-1, 4))
+    e, lm = _u32(p["extf"], (-1, 2)), _f32(p["lmt"], (3,))
+    check(load().vfr_write_mesh_cache(path.encode(), ptr(v), v.shape[0], ptr(t), ptr(c),
+                                      t.shape[0], ptr(e), e.shape[0], ptr(lm)), what=path)
+
+
+def read_mesh_cache(path) -> dict:
+    """A prepared mesh back from the binary cache (the dict ``prepare`` gives)."""
+    L = load()
+    nv, nt, ne = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    check(L.vfr_read_mesh_cache(path.encode(), None, C.byref(nv), None, None, C.byref(nt), None,
+                                C.byref(ne), None), what=path)
+    v = np.empty((nv.value, 4), np.float32)
+    t = np.empty((nt.value, 4), np.uint32)
+    c = np.empty((nt.value, 4), np.uint32)
+    e = np.empty((ne.value, 2), np.uint32)
+    lm = np.empty(3, np.float32)
+    check(L.vfr_read_mesh_cache(path.encode(), ptr(v), C.byref(nv), ptr(t), ptr(c), C.byref(nt),
+                                ptr(e), C.byref(ne), ptr(lm)), what=path)
+    return dict(vert=v, tet=t, con=c, extf=e, lmt=lm)
 
 
 def write_off(path, vert, tet):

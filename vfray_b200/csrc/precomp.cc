@@ -151,6 +151,98 @@ struct TextFile {
   }
 };
 
+// Whitespace-separated tokens after the .off header: the first nf are
+// floats (strtof, as the reference's operator>> reads them), the next nu
+// unsigned integers; anything after them is ignored, as a sequential read
+// would.  Large files are cut into chunks at whitespace; a first pass counts
+// each chunk's tokens, a second parses them into place, one thread per chunk.
+bool parse_u32_token(const char* s, const char* e, uint32_t& out) {
+  if (s == e) return false;
+  unsigned long long x = 0;
+  for (const char* c = s; c < e; ++c) {
+    if (*c < '0' || *c > '9') return false;
+    x = x * 10 + (unsigned)(*c - '0');
+    if (x > 0xffffffffull) return false;
+  }
+  out = (uint32_t)x;
+  return true;
+}
+
+inline bool is_ws(char c) { return c == ' ' || c == '\n' || c == '\t' || c == '\r'; }
+
+bool parse_tokens(const char* buf, size_t len, float* fo, size_t nf, uint32_t* uo, size_t nu) {
+  const size_t want = nf + nu;
+  const int T = (len < (64u << 20)) ? 1 : std::min(hw_threads(0), 32);
+  std::vector<size_t> cut(T + 1, len);
+  cut[0] = 0;
+  for (int t = 1; t < T; ++t) {
+    size_t c = std::max(cut[t - 1], len * (size_t)t / (size_t)T);
+    while (c < len && !is_ws(buf[c])) ++c;
+    cut[t] = c;
+  }
+  std::vector<size_t> count(T, 0);
+  auto count_chunk = [&](int t) {
+    size_t n = 0;
+    bool in = false;
+    for (size_t i = cut[t]; i < cut[t + 1]; ++i) {
+      const bool w = is_ws(buf[i]);
+      if (!w && !in) ++n;
+      in = !w;
+    }
+    count[t] = n;
+  };
+  std::vector<char> bad(T, 0);
+  std::vector<size_t> first(T + 1, 0);
+  auto parse_chunk = [&](int t) {
+    size_t k = first[t];
+    size_t i = cut[t];
+    char tmp[64];
+    while (i < cut[t + 1] && k < want) {
+      while (i < cut[t + 1] && is_ws(buf[i])) ++i;
+      if (i >= cut[t + 1]) break;
+      size_t j = i;
+      while (j < cut[t + 1] && !is_ws(buf[j])) ++j;
+      if (k < nf) {
+        const size_t n = std::min<size_t>(j - i, sizeof tmp - 1);
+        std::memcpy(tmp, buf + i, n);
+        tmp[n] = '\0';
+        char* e;
+        fo[k] = std::strtof(tmp, &e);
+        if (e == tmp) { bad[t] = 1; return; }
+      } else if (!parse_u32_token(buf + i, buf + j, uo[k - nf])) {
+        bad[t] = 1;
+        return;
+      }
+      ++k;
+      i = j;
+    }
+  };
+  auto run = [&](auto&& fn) {
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; ++t) th.emplace_back(fn, t);
+    fn(0);
+    for (auto& x : th) x.join();
+  };
+  run(count_chunk);
+  for (int t = 0; t < T; ++t) first[t + 1] = first[t] + count[t];
+  if (first[T] < want) return false;
+  run(parse_chunk);
+  for (int t = 0; t < T; ++t)
+    if (bad[t]) return false;
+  return true;
+}
+
+// Binary mesh cache: this header, then vert4 (16 B each), tet4, con4 (16 B
+// each) and extf2 (8 B each), native byte order.
+constexpr char kCacheMagic[8] = {'V', 'F', 'R', 'M', 'E', 'S', 'H', '1'};
+struct CacheHeader {
+  char magic[8];
+  uint32_t nV = 0, nT = 0, nExt = 0;
+  float lmt[3] = {0, 0, 0};
+  uint32_t reserved[2] = {0, 0};
+};
+static_assert(sizeof(CacheHeader) == 40, "cache header layout");
+
 int write_text(const char* path, const std::string& s) {
   FILE* f = std::fopen(path, "w");
   if (!f) return VFR_ERR_IO;
@@ -370,17 +462,73 @@ int vfr_default_tf(float* tf) {
 
 int vfr_read_off(const char* path, float* v, uint32_t* nV, uint32_t* tet, uint32_t* nT) {
   if (!path || !nV || !nT) return VFR_ERR_INVALID;
+  if (!v || !tet) {  // sizes only: the header line is enough
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return VFR_ERR_IO;
+    unsigned long long a = 0, b = 0;
+    const int got = std::fscanf(fp, "%llu %llu", &a, &b);
+    std::fclose(fp);
+    if (got != 2 || a > 0xffffffffull || b > 0xffffffffull) return VFR_ERR_IO;
+    *nV = (uint32_t)a;
+    *nT = (uint32_t)b;
+    return VFR_OK;
+  }
   TextFile f(path);
   if (!f.ok) return VFR_ERR_IO;
   uint32_t a, b;
   if (!f.next_u32(a) || !f.next_u32(b)) return VFR_ERR_IO;
-  if (!v || !tet) { *nV = a; *nT = b; return VFR_OK; }
   if (*nV < a || *nT < b) return VFR_ERR_INVALID;
-  for (size_t i = 0; i < 4 * (size_t)a; ++i)
-    if (!f.next_f32(v[i])) return VFR_ERR_IO;
-  for (size_t i = 0; i < 4 * (size_t)b; ++i)
-    if (!f.next_u32(tet[i])) return VFR_ERR_IO;
+  if (!parse_tokens(f.data.c_str() + f.pos, f.data.size() - 1 - f.pos, v, 4 * (size_t)a, tet,
+                    4 * (size_t)b))
+    return VFR_ERR_IO;
   *nV = a; *nT = b;
+  return VFR_OK;
+}
+
+int vfr_write_mesh_cache(const char* path, const float* vert4, uint32_t nV, const uint32_t* tet4,
+                         const uint32_t* con4, uint32_t nT, const uint32_t* extf2, uint32_t nExt,
+                         const float* lmt3) {
+  if (!path || !vert4 || !tet4 || !con4 || (!extf2 && nExt) || !lmt3) return VFR_ERR_INVALID;
+  CacheHeader h;
+  std::memcpy(h.magic, kCacheMagic, 8);
+  h.nV = nV; h.nT = nT; h.nExt = nExt;
+  std::memcpy(h.lmt, lmt3, sizeof h.lmt);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return VFR_ERR_IO;
+  bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 &&
+            std::fwrite(vert4, 16, nV, f) == nV && std::fwrite(tet4, 16, nT, f) == nT &&
+            std::fwrite(con4, 16, nT, f) == nT && std::fwrite(extf2, 8, nExt, f) == nExt;
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? VFR_OK : VFR_ERR_IO;
+}
+
+int vfr_read_mesh_cache(const char* path, float* vert4, uint32_t* nV, uint32_t* tet4,
+                        uint32_t* con4, uint32_t* nT, uint32_t* extf2, uint32_t* nExt,
+                        float* lmt3) {
+  if (!path || !nV || !nT || !nExt) return VFR_ERR_INVALID;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return VFR_ERR_IO;
+  CacheHeader h;
+  bool ok = std::fread(&h, sizeof h, 1, f) == 1 && std::memcmp(h.magic, kCacheMagic, 8) == 0;
+  if (ok) {  // the file must hold exactly the arrays its header names
+    std::fseek(f, 0, SEEK_END);
+    const long long len = std::ftell(f);
+    ok = len == (long long)(sizeof h + 16ull * h.nV + 32ull * h.nT + 8ull * h.nExt);
+    std::fseek(f, (long)sizeof h, SEEK_SET);
+  }
+  if (!ok) { std::fclose(f); return VFR_ERR_IO; }
+  if (!vert4 || !tet4 || !con4 || !lmt3 || (!extf2 && h.nExt)) {
+    std::fclose(f);
+    *nV = h.nV; *nT = h.nT; *nExt = h.nExt;
+    return VFR_OK;
+  }
+  if (*nV < h.nV || *nT < h.nT || *nExt < h.nExt) { std::fclose(f); return VFR_ERR_INVALID; }
+  ok = std::fread(vert4, 16, h.nV, f) == h.nV && std::fread(tet4, 16, h.nT, f) == h.nT &&
+       std::fread(con4, 16, h.nT, f) == h.nT && std::fread(extf2, 8, h.nExt, f) == h.nExt;
+  std::fclose(f);
+  if (!ok) return VFR_ERR_IO;
+  std::memcpy(lmt3, h.lmt, sizeof h.lmt);
+  *nV = h.nV; *nT = h.nT; *nExt = h.nExt;
   return VFR_OK;
 }
 

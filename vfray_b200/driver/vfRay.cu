@@ -11,7 +11,9 @@
 // directory, default ../tet_offs/), --size WxH, --psi FILE (a
 // psiGammaTable512.h-style table; default: the library's generated table),
 // --mode ref|composited, --device N, --out FILE.ppm, --rgba FILE (raw
-// float32 RGBA), --steps FILE (raw uint32 steps per pixel).
+// float32 RGBA), --steps FILE (raw uint32 steps per pixel), --cache (read
+// the normalised mesh, conTet, external faces and limits from <volume>.vfrb
+// when present, else read the text files as above and write that cache).
 //
 // Host-only code: the GPU work happens behind the C ABI.  Unlike the
 // reference there is no GLUT viewer (display needs a graphics stack); the
@@ -53,6 +55,7 @@ int main(int argc, char** argv) {
   std::string dir = "../tet_offs/", psi_path, out_path, rgba_path, steps_path;
   uint32_t W = 512, H = 512;
   int mode = VFR_MODE_REF, device = 0;
+  bool use_cache = false;
   const char* volume = nullptr;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
@@ -81,6 +84,8 @@ int main(int argc, char** argv) {
       rgba_path = need("--rgba");
     } else if (a == "--steps") {
       steps_path = need("--steps");
+    } else if (a == "--cache") {
+      use_cache = true;
     } else if (!volume && a[0] != '-') {
       volume = argv[i];
     } else {
@@ -96,75 +101,102 @@ int main(int argc, char** argv) {
   const std::string base = dir + volume;
   int rc;
 
-  // --- mesh and precomputed files (vfRay.cu:746-842) ---
-  std::string fn = base + ".off";
-  std::printf("Reading %s file\n", fn.c_str());
-  uint32_t nV = 0, nT = 0;
-  if (vfr_read_off(fn.c_str(), nullptr, &nV, nullptr, &nT) != VFR_OK) {
-    std::printf("Cannot read %s aborting!\n", fn.c_str());
-    return 1;
-  }
-  std::vector<float> vert(4 * (size_t)nV);
-  std::vector<uint32_t> tet(4 * (size_t)nT);
-  if ((rc = vfr_read_off(fn.c_str(), vert.data(), &nV, tet.data(), &nT)) != VFR_OK) {
-    std::printf("Cannot read %s aborting!\n", fn.c_str());
-    return 1;
-  }
-  std::printf("Normalizing vertices\n");
-  vfr_normalize(vert.data(), nV);
-
-  std::vector<uint32_t> con(4 * (size_t)nT);
-  uint32_t numExt = 0, conT = nT;
-  fn = base + ".con";
-  std::printf("Reading %s file\n", fn.c_str());
-  uint32_t hdrT = 0, hdrE = 0;
-  bool have = vfr_read_con(fn.c_str(), nullptr, &hdrT, &hdrE) == VFR_OK && hdrT == nT &&
-              vfr_read_con(fn.c_str(), con.data(), &conT, &numExt) == VFR_OK;
-  if (!have) {
-    std::printf("%s file not found!\n Computing conTet\n", fn.c_str());
-    if ((rc = vfr_build_con(tet.data(), nT, nV, con.data(), &numExt, 0)) != VFR_OK)
-      return die("buildCon", rc);
-    std::printf("Writing %s file\n", fn.c_str());
-    vfr_write_con(fn.c_str(), con.data(), nT, numExt);
-  }
-
-  std::vector<float> tf(1024);
-  fn = base + ".tf";
-  std::printf("Reading %s file\n", fn.c_str());
-  if (vfr_read_tf(fn.c_str(), tf.data()) != VFR_OK) {
-    std::printf("%s file not found!\n Computing TF\n", fn.c_str());
-    vfr_default_tf(tf.data());
-    std::printf("Writing %s file\n", fn.c_str());
-    vfr_write_tf(fn.c_str(), tf.data());
-  }
-
-  std::vector<uint32_t> extf;
-  fn = base + ".extf";
-  std::printf("Reading %s file\n", fn.c_str());
-  uint32_t ne = 0;
-  have = vfr_read_extf(fn.c_str(), nullptr, &ne) == VFR_OK && ne == numExt;
-  if (have) {
-    extf.resize(2 * (size_t)ne);
-    have = vfr_read_extf(fn.c_str(), extf.data(), &ne) == VFR_OK;
-  }
-  if (!have) {
-    std::printf("%s file not found!\n Computing extFaces\n", fn.c_str());
-    extf.resize(2 * (size_t)numExt);
-    if ((rc = vfr_build_extf(con.data(), nT, extf.data(), numExt, &ne)) != VFR_OK)
-      return die("buildExtF", rc);
-    std::printf("Writing %s file\n", fn.c_str());
-    vfr_write_extf(fn.c_str(), extf.data(), numExt);
-  }
-
+  // --- mesh and precomputed files (vfRay.cu:746-842), or the binary cache ---
+  std::vector<float> vert;
+  std::vector<uint32_t> tet, con, extf;
+  uint32_t nV = 0, nT = 0, numExt = 0;
   float lmt[3];
-  fn = base + ".lmt";
-  std::printf("Reading %s file\n", fn.c_str());
-  if (vfr_read_lmt(fn.c_str(), lmt) != VFR_OK) {
-    std::printf("%s file not found!\n Computing limits\n", fn.c_str());
-    vfr_build_lmt(vert.data(), nV, tet.data(), nT, lmt);
-    std::printf("Writing %s file\n", fn.c_str());
-    vfr_write_lmt(fn.c_str(), lmt);
+  std::string fn;
+  bool from_cache = false;
+  const std::string cache = base + ".vfrb";
+  std::vector<float> tf(1024);
+  auto read_tf_file = [&]() {  // .tf, read or computed and written (vfRay.cu:794-807)
+    const std::string f = base + ".tf";
+    std::printf("Reading %s file\n", f.c_str());
+    if (vfr_read_tf(f.c_str(), tf.data()) != VFR_OK) {
+      std::printf("%s file not found!\n Computing TF\n", f.c_str());
+      vfr_default_tf(tf.data());
+      std::printf("Writing %s file\n", f.c_str());
+      vfr_write_tf(f.c_str(), tf.data());
+    }
+  };
+  if (use_cache && vfr_read_mesh_cache(cache.c_str(), nullptr, &nV, nullptr, nullptr, &nT,
+                                       nullptr, &numExt, nullptr) == VFR_OK) {
+    std::printf("Reading %s (binary cache)\n", cache.c_str());
+    vert.resize(4 * (size_t)nV);
+    tet.resize(4 * (size_t)nT);
+    con.resize(4 * (size_t)nT);
+    extf.resize(2 * (size_t)numExt);
+    from_cache = vfr_read_mesh_cache(cache.c_str(), vert.data(), &nV, tet.data(), con.data(), &nT,
+                                     extf.data(), &numExt, lmt) == VFR_OK;
+    if (!from_cache) std::printf("%s unreadable, reading the text files\n", cache.c_str());
   }
+  if (!from_cache) {
+    fn = base + ".off";
+    std::printf("Reading %s file\n", fn.c_str());
+    if (vfr_read_off(fn.c_str(), nullptr, &nV, nullptr, &nT) != VFR_OK) {
+      std::printf("Cannot read %s aborting!\n", fn.c_str());
+      return 1;
+    }
+    vert.resize(4 * (size_t)nV);
+    tet.resize(4 * (size_t)nT);
+    if ((rc = vfr_read_off(fn.c_str(), vert.data(), &nV, tet.data(), &nT)) != VFR_OK) {
+      std::printf("Cannot read %s aborting!\n", fn.c_str());
+      return 1;
+    }
+    std::printf("Normalizing vertices\n");
+    vfr_normalize(vert.data(), nV);
+
+    con.resize(4 * (size_t)nT);
+    uint32_t conT = nT;
+    fn = base + ".con";
+    std::printf("Reading %s file\n", fn.c_str());
+    uint32_t hdrT = 0, hdrE = 0;
+    bool have = vfr_read_con(fn.c_str(), nullptr, &hdrT, &hdrE) == VFR_OK && hdrT == nT &&
+                vfr_read_con(fn.c_str(), con.data(), &conT, &numExt) == VFR_OK;
+    if (!have) {
+      std::printf("%s file not found!\n Computing conTet\n", fn.c_str());
+      if ((rc = vfr_build_con(tet.data(), nT, nV, con.data(), &numExt, 0)) != VFR_OK)
+        return die("buildCon", rc);
+      std::printf("Writing %s file\n", fn.c_str());
+      vfr_write_con(fn.c_str(), con.data(), nT, numExt);
+    }
+
+    read_tf_file();
+
+    fn = base + ".extf";
+    std::printf("Reading %s file\n", fn.c_str());
+    uint32_t ne = 0;
+    have = vfr_read_extf(fn.c_str(), nullptr, &ne) == VFR_OK && ne == numExt;
+    if (have) {
+      extf.resize(2 * (size_t)ne);
+      have = vfr_read_extf(fn.c_str(), extf.data(), &ne) == VFR_OK;
+    }
+    if (!have) {
+      std::printf("%s file not found!\n Computing extFaces\n", fn.c_str());
+      extf.resize(2 * (size_t)numExt);
+      if ((rc = vfr_build_extf(con.data(), nT, extf.data(), numExt, &ne)) != VFR_OK)
+        return die("buildExtF", rc);
+      std::printf("Writing %s file\n", fn.c_str());
+      vfr_write_extf(fn.c_str(), extf.data(), numExt);
+    }
+
+    fn = base + ".lmt";
+    std::printf("Reading %s file\n", fn.c_str());
+    if (vfr_read_lmt(fn.c_str(), lmt) != VFR_OK) {
+      std::printf("%s file not found!\n Computing limits\n", fn.c_str());
+      vfr_build_lmt(vert.data(), nV, tet.data(), nT, lmt);
+      std::printf("Writing %s file\n", fn.c_str());
+      vfr_write_lmt(fn.c_str(), lmt);
+    }
+    if (use_cache) {
+      std::printf("Writing %s (binary cache)\n", cache.c_str());
+      vfr_write_mesh_cache(cache.c_str(), vert.data(), nV, tet.data(), con.data(), nT, extf.data(),
+                           numExt, lmt);
+    }
+  }
+
+  if (from_cache) read_tf_file();
 
   std::printf("Volume dataset information: %s.off\n", base.c_str());
   std::printf("  # Tets: %u ; # Verts: %u\n", nT, nV);

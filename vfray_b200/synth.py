@@ -88,8 +88,13 @@ def carve(xyz: np.ndarray, tets: np.ndarray, seed: int, count: int = 16,
     """Drop tets whose centroid value of a seeded Gaussian field exceeds the
     given percentile; drop and re-index unreferenced vertices (vertex and tet
     order are otherwise preserved)."""
-    cen = xyz[tets].mean(axis=1)
-    val = gaussian_field(cen, count, seed)
+    # centroid field in chunks (the same values; bounded temporaries for
+    # meshes of 10^8 tets)
+    val = np.empty(tets.shape[0], dtype=np.float64)
+    step = 1 << 22
+    for lo in range(0, tets.shape[0], step):
+        cen = xyz[tets[lo:lo + step]].mean(axis=1)
+        val[lo:lo + step] = gaussian_field(cen, count, seed)
     keep = val <= np.percentile(val, percentile)
     tets = tets[keep]
     used = np.zeros(xyz.shape[0], dtype=bool)
