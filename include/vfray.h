@@ -314,6 +314,11 @@ VFR_API int vfr_write_ppm(const char* path, const uint8_t* rgb8, uint32_t W, uin
 /* Parse a psiGammaTable512.h-style C source ("float name[512][512] = {...}"). */
 VFR_API int vfr_read_psi_source(const char* path, float* out512x512);
 
+/* cleanTF (cleanTF.cc:13-88): converts a transfer function in the old
+ * layout (7 header lines, then 256 lines "index r g b a") into the .tf
+ * layout, byte for byte as the reference tool writes it. */
+VFR_API int vfr_clean_tf(const char* in_path, const char* out_path);
+
 /* Binary mesh cache (no counterpart in the reference, which re-parses its
  * text files on every run, vfRay.cu:745-842): the normalised vertices, tets,
  * conTet, external faces and limits in one file, read back with a few

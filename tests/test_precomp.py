@@ -180,3 +180,44 @@ def test_large_off_parsed_in_parallel_like_a_sequential_read(tmp_path):
     (tmp_path / "cut.off").write_text(text[: len(text) // 2])  # too few numbers
     with pytest.raises(vb.VfrError):
         vb.read_off(str(tmp_path / "cut.off"))
+
+
+def _old_tf_text(rng):
+    head = "".join(f"# header line {k} of the old layout\n" for k in range(7))
+    vals = rng.uniform(0, 1, (256, 4))
+    vals[::7] = np.round(vals[::7], 2)            # some short numbers
+    vals[3] = [1e-7, 0.5, 1.0, 123456.789]         # exponent forms, large values
+    rows = "".join(f"{i} " + " ".join(repr(float(x)) for x in row) + "\n"
+                   for i, row in enumerate(vals))
+    return head + rows
+
+
+def test_clean_tf_writes_the_tf_layout(tmp_path):
+    src = tmp_path / "old.off.tf"
+    src.write_text(_old_tf_text(np.random.default_rng(4)))
+    vb.clean_tf(str(src), str(tmp_path / "new.tf"))
+    tf = vb.read_tf(str(tmp_path / "new.tf"))
+    assert tf.shape == (256, 4) and np.isclose(tf[3, 3], 123457.0)
+    (tmp_path / "short.tf").write_text("\n" * 7 + "0 1 2 3 4\n")
+    with pytest.raises(vb.VfrError):
+        vb.clean_tf(str(tmp_path / "short.tf"), str(tmp_path / "x.tf"))
+
+
+@needs_ref
+def test_clean_tf_matches_reference_tool(tmp_path):
+    """The reference's own cleanTF (built from cleanTF.cc into oracle/_ref)
+    and this library's write the same bytes."""
+    import subprocess
+
+    import oracle
+
+    tool = os.path.join(os.path.dirname(oracle.__file__), "_ref", "cleanTF")
+    if not os.path.exists(tool):
+        pytest.skip("reference cleanTF not built")
+    for seed in range(3):
+        src = tmp_path / f"old{seed}.off.tf"
+        src.write_text(_old_tf_text(np.random.default_rng(seed)))
+        subprocess.run([tool, str(src), str(tmp_path / "ref.tf")], check=True,
+                       capture_output=True, timeout=60)
+        vb.clean_tf(str(src), str(tmp_path / "our.tf"))
+        assert (tmp_path / "ref.tf").read_bytes() == (tmp_path / "our.tf").read_bytes()

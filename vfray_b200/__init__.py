@@ -26,7 +26,7 @@ __all__ = [
     "normalize", "rotate", "build_con", "build_extf", "build_lmt", "psi_table", "default_tf",
     "prepare", "read_off", "read_con", "read_extf", "read_lmt", "read_tf", "write_off",
     "write_con", "write_extf", "write_lmt", "write_tf", "write_ppm", "read_psi_source",
-    "write_mesh_cache", "read_mesh_cache",
+    "write_mesh_cache", "read_mesh_cache", "clean_tf",
 ]
 
 
@@ -164,6 +164,11 @@ def read_psi_source(path):
     out = np.empty((512, 512), np.float32)
     check(load().vfr_read_psi_source(path.encode(), ptr(out)), what=path)
     return out
+
+
+def clean_tf(in_path, out_path):
+    """cleanTF: the old transfer-function layout to the .tf layout."""
+    check(load().vfr_clean_tf(in_path.encode(), out_path.encode()), what=in_path)
 
 
 def write_mesh_cache(path, p):

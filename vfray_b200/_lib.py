@@ -163,6 +163,7 @@ SIGNATURES = {
     "vfr_write_tf": (_i, [C.c_char_p, _vp]),
     "vfr_write_ppm": (_i, [C.c_char_p, _vp, _u32, _u32]),
     "vfr_read_psi_source": (_i, [C.c_char_p, _vp]),
+    "vfr_clean_tf": (_i, [C.c_char_p, C.c_char_p]),
     "vfr_write_mesh_cache": (_i, [C.c_char_p, _vp, _u32, _vp, _vp, _u32, _vp, _u32, _vp]),
     "vfr_read_mesh_cache": (_i, [C.c_char_p, _vp, C.POINTER(_u32), _vp, _vp, C.POINTER(_u32), _vp,
                                  C.POINTER(_u32), _vp]),

@@ -677,6 +677,35 @@ int vfr_write_tf(const char* path, const float* tf) {
   return write_text(path, s);
 }
 
+int vfr_clean_tf(const char* in_path, const char* out_path) {
+  if (!in_path || !out_path) return VFR_ERR_INVALID;
+  // the old layout (cleanTF.cc:31-56): 7 header lines, then 256 lines of
+  // "index r g b a", read as doubles
+  FILE* f = std::fopen(in_path, "r");
+  if (!f) return VFR_ERR_IO;
+  int lines = 0, c;
+  while (lines < 7 && (c = std::fgetc(f)) != EOF)
+    if (c == '\n') ++lines;
+  double tf[256][4];
+  bool ok = lines == 7;
+  for (int i = 0; ok && i < 256; ++i) {
+    long idx;
+    ok = std::fscanf(f, "%ld %lf %lf %lf %lf", &idx, &tf[i][0], &tf[i][1], &tf[i][2], &tf[i][3]) == 5;
+  }
+  std::fclose(f);
+  if (!ok) return VFR_ERR_IO;
+  // the .tf layout with ostream's default double formatting (cleanTF.cc:70-80)
+  std::string s = "256\n";
+  char buf[48];
+  for (int i = 0; i < 256; ++i)
+    for (int k = 0; k < 4; ++k) {
+      std::snprintf(buf, sizeof buf, "%g", tf[i][k]);
+      s += buf;
+      s += (k < 3) ? ' ' : '\n';
+    }
+  return write_text(out_path, s);
+}
+
 int vfr_write_ppm(const char* path, const uint8_t* rgb, uint32_t W, uint32_t H) {
   if (!path || !rgb) return VFR_ERR_INVALID;
   FILE* f = std::fopen(path, "w");
