@@ -91,3 +91,25 @@ def test_psi_coordinate_bracket():
         accepted += int(np.count_nonzero(fast | out))
     # the double division is needed for about one tau in a thousand
     assert accepted > 0.99 * 5 * tau.size
+
+
+def test_division_through_a_shared_reciprocal():
+    """float(RN_double(a * RN_double(1/b))) == a / b in float for every float
+    quotient in the normal range: random pairs over many binades, and pairs
+    built to put a / b next to a half-way point between floats."""
+    rng = np.random.default_rng(5)
+    n = 2_000_000
+    b = (rng.choice([-1, 1], n) * 2.0 ** rng.uniform(-40, 4, n)).astype(F32)
+    a = (rng.choice([-1, 1], n) * 2.0 ** rng.uniform(-60, 60, n)).astype(F32)
+    # near half-way points: a = RN(M * 2^k * b) with M odd, 25 bits
+    m = (rng.integers(1 << 24, 1 << 25, n) | 1).astype(np.float64)
+    k = rng.integers(-50, 10, n).astype(np.float64)
+    a2 = (m * 2.0 ** (k - 24) * b.astype(np.float64)).astype(F32)
+    for num in (a, a2):
+        with np.errstate(over="ignore", under="ignore"):
+            want = num / b                                    # IEEE float division
+            y = 1.0 / b.astype(np.float64)                    # correctly rounded reciprocal
+            got = (num.astype(np.float64) * y).astype(F32)
+        normal = np.abs(want) >= F32(2.0 ** -126)
+        assert normal.mean() > 0.9
+        assert np.array_equal(got[normal], want[normal])

@@ -68,9 +68,24 @@ __device__ __forceinline__ uint32_t sel4(uint4 v, uint32_t i) {
   return r;
 }
 
+// RN(a / b) for floats through a double reciprocal shared by every quotient
+// with the same divisor: y = __drcp_rn((double)b) is the correctly rounded
+// 1/b, so (double)a * y is within 2^-52 (relative) of a / b.  A quotient of
+// two floats in the normal range never lies within 2^-49 (relative) of a
+// half-way point between floats: with a = A 2^i, b = B 2^j (A, B odd, below
+// 2^24) and the half-way point M 2^k (M odd, at least 2^24), a - M 2^k b is
+// a nonzero multiple of 2^min(i, k+j), since A = M B is impossible.  So
+// rounding that double to float gives RN(a / b), the IEEE float division
+// the reference performs, whenever the quotient is in the normal range
+// (subnormal quotients can sit exactly half-way): the callers check that.
+__device__ __forceinline__ float div_by(float a, double recip_b) {
+  return __double2float_rn(__dmul_rn((double)a, recip_b));
+}
+
 // Cramer solve of the plane through a, b, c for z(x, y) and s(x, y)
-// (vfRayKernelCPU.cc:73-122, repeated at :380-429), same operand order.
-__device__ __forceinline__ void face_plane(float4 a, float4 b, float4 c, Plane& p) {
+// (vfRayKernelCPU.cc:73-122, repeated at :380-429), same operand order, with
+// IEEE float divisions.
+__device__ __forceinline__ void face_plane_ieee(float4 a, float4 b, float4 c, Plane& p) {
   const float c0x = a.x, c0y = b.x, c0z = c.x;
   const float c1x = a.y, c1y = b.y, c1z = c.y;
   const float cross = fsub(fmul(c0y, c1z), fmul(c1y, c0z));
@@ -95,6 +110,42 @@ __device__ __forceinline__ void face_plane(float4 a, float4 b, float4 c, Plane& 
     p.sy = fdiv(fadd(fsub(fmul(c0x, mx), fmul(tx, d0)), mz), det);
     p.sz = fdiv(fadd(fsub(fmul(c0x, -my), fmul(c1x, mz)), fmul(tx, cross)), det);
   }
+}
+
+// The same plane with the six divisions by det sharing one reciprocal
+// (div_by).  A coefficient of at least 2^-125 in magnitude is a quotient in
+// the normal range, so div_by gave it exactly.  When any coefficient is
+// smaller (zero included: rare, a face with an exactly constant depth or
+// scalar along an axis), the plane is solved again with IEEE divisions.
+__device__ __forceinline__ void face_plane(float4 a, float4 b, float4 c, Plane& p) {
+  const float c0x = a.x, c0y = b.x, c0z = c.x;
+  const float c1x = a.y, c1y = b.y, c1z = c.y;
+  const float cross = fsub(fmul(c0y, c1z), fmul(c1y, c0z));
+  float det = fadd(fsub(fmul(c0x, fsub(c1y, c1z)), fmul(c1x, fsub(c0y, c0z))), cross);
+  det = below_rdelta(det) ? (float)kRDelta : det;
+  const double rdet = __drcp_rn((double)det);
+  const float d1 = fsub(c1y, c1z), d0 = fsub(c0y, c0z);
+  {
+    const float tx = a.z, ty = b.z, tz = c.z;
+    const float mx = fsub(ty, tz);
+    const float my = fsub(fmul(ty, c1z), fmul(c1y, tz));
+    const float mz = fsub(fmul(c0y, tz), fmul(ty, c0z));
+    p.zx = div_by(fadd(fsub(fmul(tx, d1), fmul(c1x, mx)), my), rdet);
+    p.zy = div_by(fadd(fsub(fmul(c0x, mx), fmul(tx, d0)), mz), rdet);
+    p.zz = div_by(fadd(fsub(fmul(c0x, -my), fmul(c1x, mz)), fmul(tx, cross)), rdet);
+  }
+  {
+    const float tx = a.w, ty = b.w, tz = c.w;
+    const float mx = fsub(ty, tz);
+    const float my = fsub(fmul(ty, c1z), fmul(c1y, tz));
+    const float mz = fsub(fmul(c0y, tz), fmul(ty, c0z));
+    p.sx = div_by(fadd(fsub(fmul(tx, d1), fmul(c1x, mx)), my), rdet);
+    p.sy = div_by(fadd(fsub(fmul(c0x, mx), fmul(tx, d0)), mz), rdet);
+    p.sz = div_by(fadd(fsub(fmul(c0x, -my), fmul(c1x, mz)), fmul(tx, cross)), rdet);
+  }
+  const float m = fminf(fminf(fminf(fabsf(p.zx), fabsf(p.zy)), fminf(fabsf(p.zz), fabsf(p.sx))),
+                        fminf(fabsf(p.sy), fabsf(p.sz)));
+  if (!(m >= 0x1p-125f)) face_plane_ieee(a, b, c, p);
 }
 
 // a*x + b*y + c, left to right, no FMA

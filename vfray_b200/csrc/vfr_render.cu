@@ -613,6 +613,9 @@ int vfr_mesh_upload(vfr_ctx* c, const float* vert4, uint32_t nV, const uint32_t*
   if (!vert4 || !tet4 || !con4 || (!extf2 && nExt) || !mesh_id || nV == 0 || nT == 0)
     return C.fail(VFR_ERR_INVALID, "mesh arrays missing or empty");
   if ((uint64_t)nExt > 4ull * nT) return C.fail(VFR_ERR_INVALID, "more external faces than faces");
+  // the traversal divides depth steps (at least 1e-12) by it through a
+  // reciprocal, exact while no quotient falls below 2^-126
+  if (!(maxEdge < 0x1p80f)) return C.fail(VFR_ERR_INVALID, "maxEdgeLength not below 2^80");
   std::string why;
   if (!vfr::validate_mesh(tet4, con4, nV, nT, extf2, nExt, why)) return C.fail(VFR_ERR_MESH, why);
   std::vector<uint32_t> walk(8 * (size_t)nT);

@@ -71,7 +71,7 @@ struct Ray {
   const WalkRec* walk;         // this job's mesh and view vertices
   const float4* vert;
   uint32_t j, nT, cap;
-  float maxEdge;
+  double rmaxEdge;             // 1 / maxEdgeLength, correctly rounded (div_by)
   uint32_t cbi;                // colorBack: its transfer-function entry
   uint32_t t, f, p, iters;
   float ox, oy, zp, sp;
@@ -189,7 +189,10 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   dz = dz < 0.0f ? -dz : dz;
   dz = below_rdelta(dz) ? 0.0f : dz;
   if ((sn < 0.0f) || (sn > 1.0f)) return kSegmentEnd;  // :446
-  dz = (dz == 0.0f) ? 0.0f : fdiv(dz, R.maxEdge);
+  // dz /= maxEdgeLength (:450): dz is 0 or at least 1e-12 and maxEdgeLength
+  // below 2^80 (checked at upload; view set-up gives at most 2 sqrt 3), so
+  // the quotient is never subnormal and div_by is exact
+  dz = div_by(dz, R.rmaxEdge);
   const uint32_t tfi = (uint32_t)fmul(255.0f, sn);  // colorFront (:452)
   const float taux = fmul(S.a[tfi], dz), tauy = fmul(S.a[R.cbi], dz);
   {
@@ -299,7 +302,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
           R.vert = J.vert;
           R.nT = J.nT;
           R.cap = P.step_cap ? P.step_cap : min(4u * J.nT + 64u, 0x7fffffffu);
-          R.maxEdge = job_maxedge(J);
+          R.rmaxEdge = __drcp_rn((double)job_maxedge(J));
           R.p = J.rays[g - P.ray_pref[j]];
           const uint32_t x = R.p % J.W, y = R.p / J.W;
           R.ox = obj_coord(x, J.W);
