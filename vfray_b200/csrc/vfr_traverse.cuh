@@ -25,22 +25,27 @@ namespace vfr {
 // such multiple lies within the double rounding error of cr + 1e-12 (below
 // 2^(k-28) for multiples of 2^k) of 1e-12, whose distance to the multiples of
 // 2^-63 is 2^-67.8; for s > 2cr the difference exceeds cr > 1e-12.
+//
+// The reference swaps v1 and v2 and negates cr when cr < 0 (:323-330).  Its
+// products then become c1' = v2x v0y - v2y v0x = -c2 and c2' = -c1 exactly
+// (rounded products and differences are symmetric), and its sum and slack
+// difference are the negations of the unswapped ones.  So the swap is a sign
+// flip of (c1, c2, sum - cr): applied by xor-ing the sign of cr into them.
 __device__ __forceinline__ bool exit_test(const float4& a, const float4& b, const float4& c,
                                           float ox, float oy) {
   const float v1x = fsub(b.x, a.x), v1y = fsub(b.y, a.y);
   const float v2x = fsub(c.x, a.x), v2y = fsub(c.y, a.y);
-  float cr = fsub(fmul(v1x, v2y), fmul(v1y, v2x));
+  const float cr = fsub(fmul(v1x, v2y), fmul(v1y, v2x));
   const bool skip = below_rdelta(cr);
-  const bool neg = cr < 0.0f;
-  const float w1x = neg ? v2x : v1x, w1y = neg ? v2y : v1y;
-  const float w2x = neg ? v1x : v2x, w2y = neg ? v1y : v2y;
-  cr = neg ? -cr : cr;
   const float v0x = fsub(ox, a.x), v0y = fsub(oy, a.y);
-  const float c1 = fsub(fmul(w1x, v0y), fmul(w1y, v0x));
-  const float c2 = fsub(fmul(v0x, w2y), fmul(v0y, w2x));
-  const float sum = fadd(c1, c2);
-  const bool within = fsub(sum, cr) <= __uint_as_float(0x2b8cbcccu);
-  return !skip && (c1 >= 0.0f) && (c2 >= 0.0f) && within;
+  const float c1 = fsub(fmul(v1x, v0y), fmul(v1y, v0x));
+  const float c2 = fsub(fmul(v0x, v2y), fmul(v0y, v2x));
+  const float d = fsub(fadd(c1, c2), cr);
+  const uint32_t sg = __float_as_uint(cr) & 0x80000000u;
+  const float c1s = __uint_as_float(__float_as_uint(c1) ^ sg);
+  const float c2s = __uint_as_float(__float_as_uint(c2) ^ sg);
+  const float ds = __uint_as_float(__float_as_uint(d) ^ sg);
+  return !skip && (c1s >= 0.0f) && (c2s >= 0.0f) && (ds <= __uint_as_float(0x2b8cbcccu));
 }
 
 __device__ __forceinline__ float4 pick3(uint32_t i, const float4& x1, const float4& x2,
