@@ -148,6 +148,44 @@ def test_full_size_carved_orbit_properties(renderer, oracle_lib):
         renderer.release_mesh(mid)
 
 
+@pytest.mark.parametrize("seed,carved", [(0, False), (1, True), (2, True)])
+def test_permuted_tet_vertex_order(seed, carved, renderer, oracle_lib):
+    """Tets listing their vertices in random orders, so neighbouring tets
+    share faces under every vertex permutation (lattice meshes only ever
+    give the identity): every permutation code of the walk records runs,
+    mixed within warps.  Bit-exact steps, colour within tolerance,
+    in the single-view and the batched path."""
+    from vfray_b200 import batch as vbatch
+
+    vert, tet = synth.make_mesh(10, carved=carved, view_seed=seed + 7)
+    tet = synth.permute_tet_vertices(tet, seed)
+    p = vb.prepare(vert, tet)
+    p["tf"], p["psi"] = synth.transfer_function(seed), vb.psi_table()
+    mid = upload(renderer, p)
+    try:
+        m = oracle_lib.mesh(p["vert"], p["tet"], p["con"], p["extf"], p["tf"], p["psi"],
+                            p["lmt"][0])
+        o = oracle_lib.render_ref(m, 96, 80)
+        g = renderer.render(mid, 96, 80)
+        assert np.array_equal(g["steps"], o["steps"])
+        assert_colour(g["rgb8"], o["rgb8"], g["rgba"], o["rgba"])
+        mv = synth.orbit_views(3, seed=seed)[1]
+        single = renderer.render(mid, 64, 72, mv=mv)
+        B = vbatch.BatchRenderer(renderer, [(mid, None, 96, 80), (mid, mv, 64, 72)])
+        try:
+            B.prepare()
+            B.run()
+            B.stats()
+            steps = np.empty(96 * 80 + 64 * 72, np.uint32)
+            B.read(steps=steps)
+            assert np.array_equal(steps[:96 * 80].reshape(80, 96), o["steps"])
+            assert np.array_equal(steps[96 * 80:].reshape(72, 64), single["steps"])
+        finally:
+            B.close()
+    finally:
+        renderer.release_mesh(mid)
+
+
 @pytest.mark.parametrize("W,H", [(2, 2), (37, 23), (8, 300)])
 def test_ragged_image_sizes(W, H, renderer, oracle_lib):
     d = load_golden("convex6_rot")

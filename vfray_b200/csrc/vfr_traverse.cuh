@@ -79,7 +79,7 @@ struct Ray {
   double rmaxEdge;             // 1 / maxEdgeLength, correctly rounded (div_by)
   uint32_t cbi;                // colorBack: its transfer-function entry
   uint32_t t, f, p, iters;
-  float ox, oy, zp, sp;
+  float ox, oy, zp;
   float ar, ag, ab, tr, lastZ;
   // composited mode: this pixel's entry list and the last entry taken
   uint32_t ea, en, dz_bits, de;
@@ -109,7 +109,6 @@ __device__ __forceinline__ void begin_segment(const JobDev& J, Ray& R, uint32_t 
   R.r2 = __ldg(R.vert + sel4(id, (R.f + 2) & 3u));
   R.r3 = __ldg(R.vert + sel4(id, (R.f + 3) & 3u));
   R.zp = zp;
-  R.sp = sp;
   R.lastZ = zp;
   R.cbi = (uint32_t)fmul(255.0f, sp);
 }
@@ -225,7 +224,15 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   // advance to tn through its face fn: slots fn..fn+2 are the exit face's
   // vertices in tn's order (permutation code), slot fn+3 is the loaded vertex
   const uint32_t fn = (q >> 27) & 3u, code = q >> 29;
-  if (code < 6) {
+  if (__all_sync(__activemask(), code == 0)) {
+    // the whole warp enters through faces that keep the exit face's vertex
+    // order (permutation 012: meshes whose tets list their vertices in a
+    // consistent order, such as lattice-built ones), no selects needed
+    R.r0 = a;
+    R.r1 = b;
+    R.r2 = c;
+    R.r3 = nv;
+  } else if (code < 6) {
     const uint32_t pc = perm_code(code);
     const uint32_t m0 = pc & 3u, m1 = (pc >> 2) & 3u, m2 = (pc >> 4) & 3u;
     R.r0 = m0 == 0 ? a : (m0 == 1 ? b : c);
@@ -243,7 +250,6 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   R.t = tn;
   R.f = fn;
   R.zp = zn;
-  R.sp = sn;
   return kContinue;
 }
 

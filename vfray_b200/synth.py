@@ -31,7 +31,7 @@ import numpy as np
 __all__ = [
     "freudenthal_mesh", "gaussian_field", "carve", "transfer_function",
     "random_rotation", "orbit_views", "rotate_points", "make_mesh",
-    "write_off", "write_tf",
+    "write_off", "write_tf", "permute_tet_vertices",
 ]
 
 # The 6 Freudenthal tets of a unit cell: a monotone lattice path from corner
@@ -174,6 +174,17 @@ def make_mesh(n: int, carved: bool = False, view_seed: int | None = 3,
     vert4[:, :3] = xyz
     vert4[:, 3] = s
     return vert4, np.ascontiguousarray(tets, dtype=np.uint32)
+
+
+def permute_tet_vertices(tets: np.ndarray, seed: int) -> np.ndarray:
+    """The same tets, each listing its 4 vertices in a seeded random order.
+    Lattice-built tets list theirs in increasing id order, so a face shared
+    by two tets appears in both in the same order; real meshes need not.
+    Face order drives the exact arithmetic of the render, so tests use this
+    to cover every vertex permutation between neighbouring tets."""
+    rng = np.random.default_rng(seed)
+    order = np.argsort(rng.random(tets.shape), axis=1)
+    return np.ascontiguousarray(np.take_along_axis(tets, order, axis=1), dtype=np.uint32)
 
 
 def write_off(path: str, vert4: np.ndarray, tets: np.ndarray) -> None:
