@@ -224,20 +224,20 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   // advance to tn through its face fn: slots fn..fn+2 are the exit face's
   // vertices in tn's order (permutation code), slot fn+3 is the loaded vertex
   const uint32_t fn = (q >> 27) & 3u, code = q >> 29;
-  if (__all_sync(__activemask(), code == 0)) {
-    // the whole warp enters through faces that keep the exit face's vertex
-    // order (permutation 012: meshes whose tets list their vertices in a
-    // consistent order, such as lattice-built ones), no selects needed
-    R.r0 = a;
-    R.r1 = b;
-    R.r2 = c;
-    R.r3 = nv;
-  } else if (code < 6) {
+  if (code < 6) {
+    // per component two selects (a struct-wide select compiles to branches)
     const uint32_t pc = perm_code(code);
-    const uint32_t m0 = pc & 3u, m1 = (pc >> 2) & 3u, m2 = (pc >> 4) & 3u;
-    R.r0 = m0 == 0 ? a : (m0 == 1 ? b : c);
-    R.r1 = m1 == 0 ? a : (m1 == 1 ? b : c);
-    R.r2 = m2 == 0 ? a : (m2 == 1 ? b : c);
+    const bool b0 = (pc & 3u) == 1u, c0 = (pc & 3u) == 2u;
+    const bool b1 = ((pc >> 2) & 3u) == 1u, c1 = ((pc >> 2) & 3u) == 2u;
+    const bool b2 = ((pc >> 4) & 3u) == 1u, c2 = ((pc >> 4) & 3u) == 2u;
+#define VFR_PICK(bb, cc, k) ((cc) ? c.k : ((bb) ? b.k : a.k))
+    R.r0 = make_float4(VFR_PICK(b0, c0, x), VFR_PICK(b0, c0, y), VFR_PICK(b0, c0, z),
+                       VFR_PICK(b0, c0, w));
+    R.r1 = make_float4(VFR_PICK(b1, c1, x), VFR_PICK(b1, c1, y), VFR_PICK(b1, c1, z),
+                       VFR_PICK(b1, c1, w));
+    R.r2 = make_float4(VFR_PICK(b2, c2, x), VFR_PICK(b2, c2, y), VFR_PICK(b2, c2, z),
+                       VFR_PICK(b2, c2, w));
+#undef VFR_PICK
     R.r3 = nv;
   } else {  // shared face not matched by vertex ids: reload the tet's vertices
     const uint4 id = __ldg(P.jobs[R.j].tet + tn);
