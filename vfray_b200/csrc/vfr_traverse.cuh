@@ -48,12 +48,13 @@ __device__ __forceinline__ bool exit_test(const float4& a, const float4& b, cons
   return !skip && (c1s >= 0.0f) && (c2s >= 0.0f) && (ds <= __uint_as_float(0x2b8cbcccu));
 }
 
+// x1, x2 or x3 by i (1, 2, otherwise 3), component by component (selects,
+// no branches)
 __device__ __forceinline__ float4 pick3(uint32_t i, const float4& x1, const float4& x2,
                                         const float4& x3) {
-  float4 r = x3;
-  if (i == 1) r = x1;
-  if (i == 2) r = x2;
-  return r;
+  const bool p1 = i == 1, p2 = i == 2;
+  return make_float4(p1 ? x1.x : (p2 ? x2.x : x3.x), p1 ? x1.y : (p2 ? x2.y : x3.y),
+                     p1 ? x1.z : (p2 ? x2.z : x3.z), p1 ? x1.w : (p2 ? x2.w : x3.w));
 }
 __device__ __forceinline__ uint32_t pick3u(uint32_t i, uint32_t x1, uint32_t x2, uint32_t x3) {
   return i == 1 ? x1 : (i == 2 ? x2 : x3);
