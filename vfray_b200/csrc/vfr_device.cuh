@@ -212,22 +212,28 @@ __device__ __forceinline__ bool entry_inside(const EntryEdges& E, float ox, floa
 // the reference's.  The other cases take the double division, as written
 // in the reference.  floor(tc * 512) for tc in [0, 1] is read off
 // RD(tc * 512 + 2^23) (tc * 512 is exact), which needs no conversion unit.
-__device__ __forceinline__ int psi_coord(float tau) {
-  if (tau == 0.0f) return 0;  // gamma = 0, tc = 2^-10
-  if (tau > 0.0f && tau < 1048576.0f) {
-    const float g = __fdividef(tau, fadd(1.0f, tau));
-    const float tlo = fadd(__fsub_rd(g, 0x1p-20f), 0x1p-10f);
-    const float thi = fadd(__fadd_ru(g, 0x1p-20f), 0x1p-10f);
-    const float flo = __fmaf_rd(tlo, 512.0f, 0x1p23f);
-    const float fhi = __fmaf_rd(thi, 512.0f, 0x1p23f);
-    if (thi <= 1.0f && flo == fhi) return (int)min(__float_as_uint(flo) - 0x4b000000u, 511u);
-    if (tlo > 1.0f) return -1;
-  }
+static __device__ __noinline__ int psi_coord_double(float tau) {
   const double t = (double)tau;
-  const float g = (float)ddiv(t, dadd(1.0, t));
+  const float g = t == 0.0 ? 0.0f : (float)ddiv(t, dadd(1.0, t));
   const float tc = fadd(g, 0.5f / 512.0f);  // one float rounding either way
   if ((tc < 0.0f) || (tc > 1.0f)) return -1;
   return (int)min((uint32_t)fmul(tc, 512.0f), 511u);
+}
+
+__device__ __forceinline__ int psi_coord(float tau) {
+  // the bracket, computed for every tau (tau = 0 gives coordinate 0 here,
+  // as gamma = 0 and tc = 2^-10 do in the reference); only its verdict
+  // depends on the domain 0 <= tau < 2^20
+  const float g = __fdividef(tau, fadd(1.0f, tau));
+  const float tlo = fadd(__fsub_rd(g, 0x1p-20f), 0x1p-10f);
+  const float thi = fadd(__fadd_ru(g, 0x1p-20f), 0x1p-10f);
+  const float flo = __fmaf_rd(tlo, 512.0f, 0x1p23f);
+  const float fhi = __fmaf_rd(thi, 512.0f, 0x1p23f);
+  const bool out = tlo > 1.0f;
+  const bool ok = tau >= 0.0f && tau < 1048576.0f && (out || (thi <= 1.0f && flo == fhi));
+  int r = out ? -1 : (int)min(__float_as_uint(flo) - 0x4b000000u, 511u);
+  if (!ok) r = psi_coord_double(tau);
+  return r;
 }
 
 // zeta = (float)exp(x) for the double x = -(tau_f*0.5 + tau_b*0.5)
@@ -244,24 +250,25 @@ __device__ __forceinline__ int psi_coord(float tau) {
 // 2^18): those cases, and x outside [-80, 0], take the double exp.
 // e2tab holds 2^(j/64), j = 0..63, rounded to double.
 __device__ __forceinline__ float zeta_of(double x, const double* e2tab) {
-  if (x >= -80.0 && x <= 0.0) {
-    const double kShift = 0x1.8p52;  // adding 1.5 * 2^52 rounds to an integer
-    const double t = __fma_rn(x, 0x1.71547652b82fep+6 /* 64 / ln2 */, kShift);
-    const int k = __double2loint(t);  // round(x * 64 / ln2), -7400 <= k <= 0
-    const double kd = dsub(t, kShift);
-    double r = __fma_rn(-kd, 0x1.62e42fefa39efp-7, x);   // ln2/64, leading part
-    r = __fma_rn(-kd, 0x1.abc9e3b39803fp-62, r);         // ln2/64, trailing part
-    double p = __fma_rn(r, 1.0 / 24.0, 1.0 / 6.0);
-    p = __fma_rn(p, r, 0.5);
-    p = __fma_rn(p, r, 1.0);
-    p = __fma_rn(p, r, 1.0);
-    double e = dmul(e2tab[k & 63], p);
-    // times 2^(k >> 6): the exponent field stays far above the subnormals
-    e = __hiloint2double(__double2hiint(e) + (k >> 6) * (1 << 20), __double2loint(e));
-    const uint32_t dropped = (uint32_t)__double2loint(e) & 0x1fffffffu;
-    if (dropped - (0x10000000u - 1024u) > 2048u) return (float)e;
-  }
-  return (float)exp(x);
+  // computed for every x (e2tab is indexed in range whatever x is); only
+  // the verdict depends on the domain -80 <= x <= 0
+  const double kShift = 0x1.8p52;  // adding 1.5 * 2^52 rounds to an integer
+  const double t = __fma_rn(x, 0x1.71547652b82fep+6 /* 64 / ln2 */, kShift);
+  const int k = __double2loint(t);  // round(x * 64 / ln2), -7400 <= k <= 0 in the domain
+  const double kd = dsub(t, kShift);
+  double r = __fma_rn(-kd, 0x1.62e42fefa39efp-7, x);   // ln2/64, leading part
+  r = __fma_rn(-kd, 0x1.abc9e3b39803fp-62, r);         // ln2/64, trailing part
+  double p = __fma_rn(r, 1.0 / 24.0, 1.0 / 6.0);
+  p = __fma_rn(p, r, 0.5);
+  p = __fma_rn(p, r, 1.0);
+  p = __fma_rn(p, r, 1.0);
+  double e = dmul(e2tab[k & 63], p);
+  // times 2^(k >> 6): the exponent field stays far above the subnormals
+  e = __hiloint2double(__double2hiint(e) + (k >> 6) * (1 << 20), __double2loint(e));
+  const uint32_t dropped = (uint32_t)__double2loint(e) & 0x1fffffffu;
+  float z = (float)e;
+  if (!(x >= -80.0 && x <= 0.0 && dropped - (0x10000000u - 1024u) > 2048u)) z = (float)exp(x);
+  return z;
 }
 
 // Orderable encoding of floats for atomicMin/atomicMax on unsigned ints.
