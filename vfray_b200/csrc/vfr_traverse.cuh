@@ -162,23 +162,27 @@ __device__ __forceinline__ void finish_pixel(const JobDev& J, const Ray& R) {
 
 enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kAbandon = 2, kCap = 3, kRange = 4 };
 
-// One iteration of the reference's while loop (:302-542).
+// One iteration of the reference's while loop (:302-542).  The ways it can
+// end before compositing (step cap, no exit face, id range, scalar or psi
+// coordinate out of range) are folded into a status and the arithmetic runs
+// on for every lane; the ray's state is only committed while the status
+// says to go on, so no lane takes an early branch.
 __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTables& S, Ray& R) {
-  if (++R.iters > R.cap) return kCap;
+  uint32_t st = (++R.iters > R.cap) ? kCap : kContinue;
   const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
   const bool h3 = exit_test(R.r3, R.r0, R.r1, R.ox, R.oy);
   const uint32_t i = h1 ? 1u : (h2 ? 2u : (h3 ? 3u : 0u));
-  if (i == 0) return kSegmentEnd;  // :353 no exit face
+  st = (st == kContinue && i == 0) ? kSegmentEnd : st;  // :353 no exit face
   const uint32_t ex = (R.f + i) & 3u;
   const uint32_t tn = sel4(R.w.n, ex);
   const uint32_t q = sel4(R.w.q, ex);
   const bool leaving = (tn == R.t);
-  if (tn >= R.nT) return kRange;
+  st = (st == kContinue && tn >= R.nT) ? kRange : st;
   // both loads of the step, issued before the plane solve that hides them
   WalkRec N = R.w;
   float4 nv = R.r0;
-  if (!leaving) {
+  if (st == kContinue && !leaving) {
     N = ldg_walk(R.walk, tn);
     nv = __ldg(R.vert + (q & 0x07ffffffu));
   }
@@ -193,18 +197,18 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   float dz = fsub(R.zp, zn);
   dz = dz < 0.0f ? -dz : dz;
   dz = below_rdelta(dz) ? 0.0f : dz;
-  if ((sn < 0.0f) || (sn > 1.0f)) return kSegmentEnd;  // :446
+  st = (st == kContinue && ((sn < 0.0f) || (sn > 1.0f))) ? kSegmentEnd : st;  // :446
   // dz /= maxEdgeLength (:450): dz is 0 or at least 1e-12 and maxEdgeLength
   // below 2^80 (checked at upload; view set-up gives at most 2 sqrt 3), so
   // the quotient is never subnormal and div_by is exact
   dz = div_by(dz, R.rmaxEdge);
-  const uint32_t tfi = (uint32_t)fmul(255.0f, sn);  // colorFront (:452)
+  const uint32_t tfi = min((uint32_t)fmul(255.0f, sn), 255u);  // colorFront (:452)
   const float taux = fmul(S.a[tfi], dz), tauy = fmul(S.a[R.cbi], dz);
   {
     const float zeta = zeta_of(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)), S.e2);
     const int ci = psi_coord(taux), cj = psi_coord(tauy);
-    if ((ci | cj) < 0) return kSegmentEnd;  // :468
-    const double psi = (double)__ldg(P.psi + (uint32_t)ci * 512u + (uint32_t)cj);
+    st = (st == kContinue && (ci | cj) < 0) ? kSegmentEnd : st;  // :468
+    const double psi = (double)__ldg(P.psi + (uint32_t)max(ci, 0) * 512u + (uint32_t)max(cj, 0));
     const double dzeta = (double)zeta;
     const double ca = dsub(1.0, psi), cbk = dsub(psi, dzeta);
     const double2 frg = S.rg[tfi], brg = S.rg[R.cbi];
@@ -214,14 +218,21 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
     const float fb = (float)dadd(dmul(fbl, ca), dmul(bbl, cbk));
     const float fw = fsub(1.0f, zeta);           // (float)(1.0 - zeta), innocuous double rounding
     const double keep = dsub(1.0, (double)fw);   // exact
-    R.ar = (float)dadd((double)fr, dmul(keep, (double)R.ar));
-    R.ag = (float)dadd((double)fg, dmul(keep, (double)R.ag));
-    R.ab = (float)dadd((double)fb, dmul(keep, (double)R.ab));
-    R.tr = fmul(R.tr, zeta);
+    const float ar = (float)dadd((double)fr, dmul(keep, (double)R.ar));
+    const float ag = (float)dadd((double)fg, dmul(keep, (double)R.ag));
+    const float ab = (float)dadd((double)fb, dmul(keep, (double)R.ab));
+    const float tr = fmul(R.tr, zeta);
+    if (st == kContinue) {
+      R.ar = ar;
+      R.ag = ag;
+      R.ab = ab;
+      R.tr = tr;
+      R.lastZ = zn;
+      R.cbi = tfi;
+      st = leaving ? kSegmentEnd : st;  // :535
+    }
   }
-  R.lastZ = zn;
-  R.cbi = tfi;
-  if (leaving) return kSegmentEnd;  // :535
+  if (st != kContinue) return st;
   // advance to tn through its face fn: slots fn..fn+2 are the exit face's
   // vertices in tn's order (permutation code), slot fn+3 is the loaded vertex
   const uint32_t fn = (q >> 27) & 3u, code = q >> 29;
