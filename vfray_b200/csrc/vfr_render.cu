@@ -977,7 +977,7 @@ int vfr_batch_autotune(vfr_batch* b, int reps, vfr_tuning* out) {
   vfr::Tuning best = saved;
   float best_ms = 1e30f;
   int rc = VFR_OK;
-  const uint32_t variants[] = {0, 1}, refills[] = {1, 4}, tiles[] = {4, 8, 16},
+  const uint32_t variants[] = {0, 1}, refills[] = {4, 6}, tiles[] = {4, 8, 16},
                  rasters[] = {16, 64};
   for (uint32_t var : variants)
     for (uint32_t rf : refills)
