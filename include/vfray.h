@@ -108,7 +108,9 @@ VFR_API int vfr_tables_upload(vfr_ctx* ctx, const float* tf256x4, const float* p
  * arrays are copied; the mesh stays resident until released.  Validates ids,
  * adjacency symmetry and the external-face list (VFR_ERR_MESH on failure:
  * the reference would walk such a mesh into its :365 `return`).  maxZ/minZ
- * are accepted for the .lmt layout; only maxEdge enters the render. */
+ * are accepted for the .lmt layout; only maxEdge enters the render, and it
+ * must be below 2^80 (VFR_ERR_INVALID otherwise; a normalised mesh has at
+ * most 2 sqrt 3).  At most 2^27 vertices. */
 VFR_API int vfr_mesh_upload(vfr_ctx* ctx, const float* vert4, uint32_t nV, const uint32_t* tet4,
                     const uint32_t* con4, uint32_t nT, const uint32_t* extf2, uint32_t nExt,
                     float maxEdge, float maxZ, float minZ, int* mesh_id);

@@ -1,10 +1,14 @@
 // Stage (c): tet-to-tet traversal with partial pre-integration
 // (vfRayKernelCPU.cc:173-566), one lane per ray, persistent warps.
 //
-// Per-lane state machine: a lane walks one tet per loop iteration; when its
-// ray ends it writes the pixel and the warp refills idle lanes from the
-// view's ray queue (one warp-aggregated atomicAdd), so lanes do not wait for
-// the longest ray of their warp.  The current tet's 4 vertices live in
+// Per-lane state machine: a lane walks up to two tets per loop pass; when its
+// ray ends it writes the pixel, and once enough lanes of the warp are idle
+// the warp refills them from the batch's single ray queue (one
+// warp-aggregated atomicAdd), so lanes do not wait for the longest ray of
+// their warp.  The kernel is bound by instruction issue, so the step is
+// written to keep lanes converged: its arithmetic is branch-free, its rare
+// exact fallbacks (psi coordinate, exp, plane re-solve) sit out of line, and
+// every way a step can end is a status rather than an early return.  The current tet's 4 vertices live in
 // registers rotated by the entry face f (r_j = local vertex (f + j) & 3), so
 // the three exit candidates (f+1, f+2, f+3) read fixed registers: candidate
 // i uses (r_i, r_i+1, r_i+2).  Once the exit face is known, a step issues its
