@@ -51,6 +51,16 @@ def test_rejects_interior_face_in_ext_list(renderer, case):
            case["lmt"])
 
 
+def test_rejects_unusable_max_edge(renderer, case):
+    """maxEdgeLength enters the traversal through a reciprocal whose quotients
+    must stay normal: values from 2^80 up, and NaN, are refused."""
+    for bad in (2.0 ** 80, float("inf"), float("nan")):
+        lmt = case["lmt"].copy()
+        lmt[0] = bad
+        expect(vb._lib.VFR_ERR_INVALID, renderer.upload_mesh, case["vert"], case["tet"],
+               case["con"], case["extf"], lmt)
+
+
 def test_stage_order_and_handles(renderer, case):
     mid = renderer.upload_mesh(case["vert"], case["tet"], case["con"], case["extf"], case["lmt"])
     try:
