@@ -86,13 +86,26 @@ __global__ void __launch_bounds__(256) view_rotate_kernel(const JobDev* __restri
       mx[k] = fmaxf(mx[k], c[k]);
     }
   }
+  // one pair of atomics per block and coordinate: warps reduce, then the
+  // block through shared memory
+  __shared__ float s_mm[8][8];
+  const uint32_t w = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const float a = warp_min(mn[k]), b = warp_max(mx[k]);
     if ((threadIdx.x & 31u) == 0) {
-      atomicMin(&J.ctr->mm[k], f2ord(a));
-      atomicMax(&J.ctr->mm[4 + k], f2ord(b));
+      s_mm[w][k] = a;
+      s_mm[w][4 + k] = b;
     }
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const uint32_t k = threadIdx.x;
+    float v = s_mm[0][k];
+    for (uint32_t i = 1; i < (blockDim.x >> 5); ++i)
+      v = k < 4 ? fminf(v, s_mm[i][k]) : fmaxf(v, s_mm[i][k]);
+    if (k < 4) atomicMin(&J.ctr->mm[k], f2ord(v));
+    else atomicMax(&J.ctr->mm[k], f2ord(v));
   }
 }
 
@@ -149,8 +162,14 @@ __global__ void __launch_bounds__(256) view_maxedge_kernel(const JobDev* __restr
       if (len > best) best = len;
     }
   }
+  __shared__ float s_best[8];
   best = warp_max(best);
-  if ((threadIdx.x & 31u) == 0) atomicMax(&J.ctr->maxedge_bits, __float_as_uint(best));
+  if ((threadIdx.x & 31u) == 0) s_best[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t i = 1; i < (blockDim.x >> 5); ++i) best = fmaxf(best, s_best[i]);
+    atomicMax(&J.ctr->maxedge_bits, __float_as_uint(best));
+  }
 }
 
 // ------------------------------------------------------------ stage (a)
