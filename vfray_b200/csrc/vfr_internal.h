@@ -36,8 +36,13 @@ struct Mesh {
   WalkRec* walk = nullptr;  // neighbour + opposite-vertex words per tet
   float4* vert = nullptr;
   uint2* extf = nullptr;
+  // the mesh's distinct edges (min id, max id), built on first use by a view
+  // with a model-view (its maxEdgeLength is recomputed per view)
+  uint2* edges = nullptr;
+  uint32_t nEdges = 0;
   size_t bytes = 0;
   ~Mesh() {
+    if (edges) cudaFree(edges);
     if (tet) cudaFree(tet);
     if (walk) cudaFree(walk);
     if (vert) cudaFree(vert);
@@ -141,6 +146,7 @@ struct Ctx {
   int cuda(cudaError_t e, const char* what);
   int grow(Buf& b, size_t bytes, const char* what);
   Mesh* mesh(int id);
+  int mesh_edges(Mesh* m, cudaStream_t st);
   int traverse_blocks_per_sm(int mode);
   const void* traverse_fn(int mode, uint32_t variant);
   int check_status(uint32_t status, uint32_t nentries_over);

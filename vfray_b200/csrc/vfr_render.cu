@@ -9,6 +9,9 @@
 // CUDA graph.  A single view is a batch of one job.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -151,6 +154,53 @@ void Batch::drop_graph() {
 
 static uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
+// The mesh's distinct edges, once per mesh: the 6 edge keys of every tet,
+// sorted (CUB radix sort over the bits the vertex ids use) and made unique.
+// Temporaries are freed before returning; the stream is synchronised.
+int Ctx::mesh_edges(Mesh* m, cudaStream_t st) {
+  if (m->edges) return VFR_OK;
+  const size_t n = 6 * (size_t)m->nT;
+  int bits = 1;
+  while (bits < 32 && (1ull << bits) < m->nV) ++bits;
+  unsigned long long *keys = nullptr, *sorted = nullptr, *uniq = nullptr;
+  unsigned long long* count = nullptr;
+  void* tmp = nullptr;
+  size_t tmp_sort = 0, tmp_uniq = 0;
+  int rc = cuda(cudaMalloc(&keys, n * 8), "edge keys");
+  if (!rc) rc = cuda(cudaMalloc(&sorted, n * 8), "edge keys");
+  if (!rc) rc = cuda(cudaMalloc(&uniq, n * 8), "edge keys");
+  if (!rc) rc = cuda(cudaMalloc(&count, sizeof(unsigned long long)), "edge count");
+  if (!rc) {
+    cub::DeviceRadixSort::SortKeys(nullptr, tmp_sort, keys, sorted, n, 0, 32 + bits, st);
+    cub::DeviceSelect::Unique(nullptr, tmp_uniq, sorted, uniq, count, n, st);
+    rc = cuda(cudaMalloc(&tmp, std::max(tmp_sort, tmp_uniq)), "edge sort scratch");
+  }
+  if (!rc) {
+    edge_keys_kernel<<<cdiv(m->nT, 256), 256, 0, st>>>(m->tet, m->nT, keys);
+    rc = cuda(cub::DeviceRadixSort::SortKeys(tmp, tmp_sort, keys, sorted, n, 0, 32 + bits, st),
+              "edge sort");
+  }
+  if (!rc) rc = cuda(cub::DeviceSelect::Unique(tmp, tmp_uniq, sorted, uniq, count, n, st), "edge unique");
+  unsigned long long ne = 0;
+  if (!rc)
+    rc = cuda(cudaMemcpyAsync(&ne, count, sizeof(ne), cudaMemcpyDeviceToHost, st), "edge count");
+  if (!rc) rc = cuda(cudaStreamSynchronize(st), "edge build");
+  if (!rc) rc = cuda(cudaMalloc(&m->edges, sizeof(uint2) * std::max<size_t>(ne, 1)), "edges");
+  if (!rc) rc = cuda(cudaMemcpyAsync(m->edges, uniq, sizeof(uint2) * ne, cudaMemcpyDeviceToDevice, st),
+                     "edges");
+  if (!rc) rc = cuda(cudaStreamSynchronize(st), "edge build");
+  for (void* p : {(void*)keys, (void*)sorted, (void*)uniq, (void*)count, tmp})
+    if (p) cudaFree(p);
+  if (rc) {
+    if (m->edges) cudaFree(m->edges);
+    m->edges = nullptr;
+    return rc;
+  }
+  m->nEdges = (uint32_t)ne;
+  m->bytes += sizeof(uint2) * ne;
+  return VFR_OK;
+}
+
 // Lays the jobs out in the batch's arenas (allocating what is missing) and
 // fills the job table on the host.
 int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
@@ -174,8 +224,13 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
       return C.fail(VFR_ERR_INVALID, "image size out of range");
     const uint32_t rb =
         q.use_mv ? std::max<uint32_t>(1, std::min<uint32_t>(cdiv(mesh->nV, 1024), 2 * C.num_sms)) : 0;
+    if (q.use_mv) {
+      const int rc = C.mesh_edges(mesh, st());
+      if (rc) return rc;
+    }
     const uint32_t eb =
-        q.use_mv ? std::max<uint32_t>(1, std::min<uint32_t>(cdiv(mesh->nT, 1024), 4 * C.num_sms)) : 0;
+        q.use_mv ? std::max<uint32_t>(1, std::min<uint32_t>(cdiv(mesh->nEdges, 1024), 4 * C.num_sms))
+                 : 0;
     const uint32_t xb = cdiv(mesh->nExt, 1024);
     const uint32_t tl = cdiv(q.W, C.tune.tile_w) * cdiv(q.H, 32 / C.tune.tile_w);
     pr[j + 1] = pr[j] + rb;
@@ -235,6 +290,8 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     J.m1 = make_float4(q.mv[4], q.mv[5], q.mv[6], q.mv[7]);
     J.m2 = make_float4(q.mv[8], q.mv[9], q.mv[10], q.mv[11]);
     J.tet = mesh->tet;
+    J.edges = mesh->edges;
+    J.nEdges = mesh->nEdges;
     J.walk = mesh->walk;
     J.vert_in = mesh->vert;
     J.extf = mesh->extf;

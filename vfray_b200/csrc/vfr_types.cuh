@@ -21,6 +21,8 @@ struct __align__(16) ViewCounters {
 struct __align__(16) JobDev {
   float4 m0, m1, m2;         // rows of the model-view (use_mv)
   const uint4* tet;          // mesh
+  const uint2* edges;        // the mesh's distinct edges (jobs with a model-view)
+  uint32_t nEdges;
   const WalkRec* walk;
   const float4* vert_in;     // the mesh's (normalised) vertices
   const uint2* extf;
