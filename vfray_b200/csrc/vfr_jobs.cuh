@@ -211,8 +211,10 @@ __global__ void __launch_bounds__(1024) visible_kernel(const JobDev* __restrict_
     const float faceZ = plane_eval(op.x, op.y, P.zx, P.zy, P.zz);
     if (faceZ < op.z) P.sx = -1.0f;  // :128 invisible sentinel
     vis = (P.sx != -1.0f);
-    J.planes[2 * (size_t)e] = make_float4(P.zx, P.zy, P.zz, P.sx);
-    J.planes[2 * (size_t)e + 1] = make_float4(P.sy, P.sz, 0.0f, 0.0f);
+    float4* pl = J.planes + kPlaneStride * (size_t)e;
+    pl[0] = make_float4(P.zx, P.zy, P.zz, P.sx);
+    pl[1] = make_float4(P.sy, P.sz, v0.x, v0.y);
+    pl[2] = make_float4(v1.x, v1.y, v2.x, v2.y);
   }
   const int cnt = __syncthreads_count(vis);
   if (threadIdx.x == 0) J.blk[lb] = (uint32_t)cnt;
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(1024) compact_kernel(const JobDev* __restrict_
   }
   __syncthreads();
   const uint32_t e = lb * blockDim.x + threadIdx.x;
-  const bool vis = e < J.nExt && J.planes[2 * (size_t)e].w != -1.0f;
+  const bool vis = e < J.nExt && J.planes[kPlaneStride * (size_t)e].w != -1.0f;
   const uint32_t m = __ballot_sync(0xffffffffu, vis);
   if (lane == 0) s_warp[warp] = __popc(m);
   __syncthreads();
@@ -332,11 +334,13 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
     const uint32_t i = g - vpref[j];
     const uint32_t W = J.W, H = J.H;
     const uint32_t e = J.vis_ext[i];
-    const uint2 tf = J.extf[e];
-    const uint4 id = J.tet[tf.x];
-    const float4 v0 = J.vert[sel4(id, tf.y & 3u)];
-    const float4 v1 = J.vert[sel4(id, (tf.y + 1) & 3u)];
-    const float4 v2 = J.vert[sel4(id, (tf.y + 2) & 3u)];
+    // the face's plane and vertex xy, written by stage (a): one dependent
+    // load after the visible list instead of the face -> tet -> vertex chain
+    const float4* pl = J.planes + kPlaneStride * (size_t)e;
+    const float4 p0 = pl[0], p1 = pl[1], p2 = pl[2];
+    const float4 v0 = make_float4(p1.z, p1.w, 0.0f, 0.0f);
+    const float4 v1 = make_float4(p2.x, p2.y, 0.0f, 0.0f);
+    const float4 v2 = make_float4(p2.z, p2.w, 0.0f, 0.0f);
     uint32_t bx = W - 1, by = H - 1, bz = 0, bw = 0;
     const float4 vv[3] = {v0, v1, v2};
 #pragma unroll
@@ -351,7 +355,6 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
     const uint32_t xe = min(bz, W - 1), ye = min(bw, H - 1);
     if (bx > xe || by > ye) continue;  // box entirely outside the image
     const EntryEdges E = entry_edges(v0, v1, v2);
-    const float4 p0 = J.planes[2 * (size_t)e], p1 = J.planes[2 * (size_t)e + 1];
     const uint32_t h = ye - by + 1;
     const uint32_t rh = h >= 32 ? 32u : (h <= 1 ? 1u : 1u << (32 - __clz(h - 1)));
     const uint32_t cw = 32u / rh;

@@ -256,7 +256,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
   if (!rc) rc = C.grow(d_dev_pref, sizeof(uint32_t) * (2 * (size_t)(njobs + 1) + 4), "device prefixes");
   if (!rc) rc = C.grow(d_ctr, sizeof(ViewCounters) * njobs, "view counters");
   if (!rc) rc = C.grow(vview, sizeof(float4) * nv_mv, "view vertices");
-  if (!rc) rc = C.grow(planes, sizeof(float4) * 2 * next, "planes");
+  if (!rc) rc = C.grow(planes, sizeof(float4) * kPlaneStride * next, "planes");
   if (!rc) rc = C.grow(blk, sizeof(uint32_t) * nblk, "block counts");
   if (!rc) rc = C.grow(vis, sizeof(uint32_t) * next, "visible lists");
   if (!rc) rc = C.grow(bbox, sizeof(uint4) * next, "bboxes");
@@ -297,7 +297,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     J.extf = mesh->extf;
     J.vview = q.use_mv ? vview.as<float4>(sizeof(float4) * ov) : nullptr;
     J.vert = q.use_mv ? J.vview : mesh->vert;
-    J.planes = planes.as<float4>(sizeof(float4) * 2 * oe);
+    J.planes = planes.as<float4>(sizeof(float4) * kPlaneStride * oe);
     J.blk = blk.as<uint32_t>(sizeof(uint32_t) * ob);
     J.vis_ext = vis.as<uint32_t>(sizeof(uint32_t) * oe);
     J.bbox = bbox.as<uint4>(sizeof(uint4) * oe);
@@ -751,11 +751,11 @@ int vfr_find_visible(vfr_ctx* c, int id, uint32_t* num_vis, uint32_t* visExt, fl
     rc = C.cuda(cudaMemcpy(visExt, J.vis_ext, sizeof(uint32_t) * k[0].nvis, cudaMemcpyDeviceToHost),
                 "visible list read");
   if (!rc && faceData && m->nExt) {
-    std::vector<float4> pl(2 * (size_t)m->nExt);
+    std::vector<float4> pl(vfr::kPlaneStride * (size_t)m->nExt);
     rc = C.cuda(cudaMemcpy(pl.data(), J.planes, sizeof(float4) * pl.size(), cudaMemcpyDeviceToHost),
                 "plane read");
     for (size_t e = 0; e < m->nExt && !rc; ++e) {
-      const float4 a = pl[2 * e], b = pl[2 * e + 1];
+      const float4 a = pl[vfr::kPlaneStride * e], b = pl[vfr::kPlaneStride * e + 1];
       float* o = faceData + 6 * e;
       o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y;
     }

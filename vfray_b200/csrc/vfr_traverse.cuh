@@ -145,7 +145,7 @@ __device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev
     R.de = be;
     first = false;
     if (bz > R.exitZ) continue;  // behind the ray already
-    const float4 p0 = J.planes[2 * (size_t)be], p1 = J.planes[2 * (size_t)be + 1];
+    const float4 p0 = J.planes[kPlaneStride * (size_t)be], p1 = J.planes[kPlaneStride * (size_t)be + 1];
     begin_segment(J, R, be, bz, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
     return true;
   }
@@ -339,7 +339,8 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
           R.iters = 0;
           if (kMode == 0) {
             const uint32_t e = (uint32_t)J.winner[R.p];
-            const float4 p0 = J.planes[2 * (size_t)e], p1 = J.planes[2 * (size_t)e + 1];
+            const float4 p0 = J.planes[kPlaneStride * (size_t)e];
+            const float4 p1 = J.planes[kPlaneStride * (size_t)e + 1];
             begin_segment(J, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
                           plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
             active = true;

@@ -28,7 +28,7 @@ struct __align__(16) JobDev {
   const uint2* extf;
   const float4* vert;        // vertices this view renders with (vert_in or vview)
   float4* vview;             // rotated + normalised vertices (use_mv)
-  float4* planes;            // 2 per external face
+  float4* planes;            // kPlaneStride per external face
   uint32_t* blk;             // visible count per block of 1024 external faces
   uint32_t* vis_ext;         // visible external faces, in order
   uint4* bbox;               // per visible face
@@ -46,6 +46,11 @@ struct __align__(16) JobDev {
   float maxEdge_in;          // the mesh's maxEdgeLength when !use_mv
   uint32_t pix_base;         // first pixel of this job in the batch's pixel arenas
 };
+
+// Face planes per external face: three float4, (zx zy zz sx | sy sz v0x v0y |
+// v1x v1y v2x v2y), the plane of findVisibleFaces (sx = -1: not visible) and
+// the xy of the face's vertices for stage (b).
+constexpr uint32_t kPlaneStride = 3;
 
 struct TraverseParams {
   const JobDev* jobs;
