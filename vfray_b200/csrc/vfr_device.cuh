@@ -154,17 +154,25 @@ __device__ __forceinline__ float plane_eval(float x, float y, float a, float b, 
 }
 
 // obj = (pix*2)/(float)(res-1) - 1.0 (vfRayKernelCPU.cc:250,254): float
-// quotient, double subtraction, stored as float.
+// quotient, then a double subtraction stored as float, which is the float
+// subtraction (q - 1 is exact in double; one rounding to float either way).
+// pix*2 < 2^24 is exact as a float.
 __device__ __forceinline__ float obj_coord(uint32_t pix, uint32_t res) {
-  float q = fdiv((float)(pix * 2u), (float)(res - 1u));
-  return (float)dsub((double)q, 1.0);
+  return fsub(fdiv((float)(pix * 2u), (float)(res - 1u)), 1.0f);
+}
+
+// The same with the division through rres = __drcp_rn((double)(float)(res-1))
+// (div_by: the quotient is 0 or at least 2/(res-1), in the normal range).
+__device__ __forceinline__ float obj_coord_r(uint32_t pix, double rres) {
+  return fsub(div_by((float)(pix * 2u), rres), 1.0f);
 }
 
 // (uint)((res - 1.0) * (x + 1.0) / 2.0) in double (vfRayKernelCPU.cc:158-159),
 // converted the way the x86-64 reference binary converts: truncate to a
 // 64-bit integer and keep the low 32 bits.
 __device__ __forceinline__ uint32_t to_pixel(float x, uint32_t res) {
-  double d = ddiv(dmul(dsub((double)res, 1.0), dadd((double)x, 1.0)), 2.0);
+  // halving is exact, so the division by 2.0 is a multiplication by 0.5
+  double d = dmul(dmul(dsub((double)res, 1.0), dadd((double)x, 1.0)), 0.5);
   return (uint32_t)(unsigned long long)__double2ll_rz(d);
 }
 

@@ -355,6 +355,7 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
     const uint32_t xe = min(bz, W - 1), ye = min(bw, H - 1);
     if (bx > xe || by > ye) continue;  // box entirely outside the image
     const EntryEdges E = entry_edges(v0, v1, v2);
+    const double rW = __drcp_rn((double)(float)(W - 1u)), rH = __drcp_rn((double)(float)(H - 1u));
     const uint32_t h = ye - by + 1;
     const uint32_t rh = h >= 32 ? 32u : (h <= 1 ? 1u : 1u << (32 - __clz(h - 1)));
     const uint32_t cw = 32u / rh;
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
     const uint32_t upto = seg & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u));   // rows <= mine
     for (uint32_t x0 = bx; x0 <= xe; x0 += cw) {
       const uint32_t px = x0 + c;
-      const float ox = obj_coord(px, W);
+      const float ox = obj_coord_r(px, rW);
       bool carried = false;  // a kill in an earlier row chunk of this column (rh == 32)
       for (uint32_t y0 = by; y0 <= ye; y0 += rh) {
         const uint32_t py = y0 + r;
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
         bool inside = false, ok = false;
         float oy = 0.0f, sp = 0.0f;
         if (live) {
-          oy = obj_coord(py, H);
+          oy = obj_coord_r(py, rH);
           inside = entry_inside(E, ox, oy);
           sp = plane_eval(ox, oy, p0.w, p1.x, p1.y);
           ok = (sp >= 0.0f) && (sp <= 1.0f);
