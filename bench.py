@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--workload", default="orbit64",
                     choices=["orbit64", "mixed", "served", "convex24", "large"])
     ap.add_argument("--views", type=int, default=64, help="orbit views (orbit64)")
+    ap.add_argument("--mode", default="ref", choices=["ref", "composited"],
+                    help="ref: the reference's last-visible-face image; composited: every "
+                         "entry segment of each ray, depth-ordered")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="bound of the CPU-baseline sample")
@@ -246,11 +249,12 @@ def run_ours(args, rank, world, dist):
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     jobs = [(mids[m], mv, W, H) for (m, mv, W, H) in wl["jobs"]]
     nj = len(jobs)
+    mode = vb.MODE_COMPOSITED if args.mode == "composited" else vb.MODE_REF
 
     # per-job rays and steps from single-view renders (checked below against the batch)
     rays_j, steps_j = [], []
     for (mid, mv, W, H) in jobs:
-        o = r.render(mid, W, H, mv=mv, rgba=False, steps=False)
+        o = r.render(mid, W, H, mv=mv, mode=mode, rgba=False, steps=False)
         rays_j.append(o["stats"]["num_rays"])
         steps_j.append(o["stats"]["num_steps"])
     rays_step, steps_step = int(sum(rays_j)), int(sum(steps_j))
@@ -261,11 +265,11 @@ def run_ours(args, rank, world, dist):
 
     def plain_step():
         for i, (mid, mv, W, H) in enumerate(jobs):
-            r.render_device(mid, W, H, mv=mv, rgb8=rgb_d[3 * offs[i]:3 * offs[i + 1]],
+            r.render_device(mid, W, H, mv=mv, mode=mode, rgb8=rgb_d[3 * offs[i]:3 * offs[i + 1]],
                             rgba=rgba_d[4 * offs[i]:4 * offs[i + 1]])
 
     tuning = None
-    runner = vbatch.BatchRenderer(r, jobs)
+    runner = vbatch.BatchRenderer(r, jobs, mode=mode)
     if not args.no_autotune:
         tuning = runner.autotune(reps=1)
     runner.prepare()
@@ -313,7 +317,7 @@ def run_ours(args, rank, world, dist):
     t_batch, _ = timed(batched_step, kp, 1)
     # stage times of the batched chain: the same batch launched directly
     # (not as a graph) with events between its stages
-    runner_p = vbatch.BatchRenderer(r, jobs, graph=False)
+    runner_p = vbatch.BatchRenderer(r, jobs, mode=mode, graph=False)
     _, prof_batch = timed(lambda: runner_p.run(), kp, 1, profile=True)
     runner_p.close()
     prof, launches_per_trav = (prof_batch, 1) if args.form == "batched" else (prof_plain, nj)
@@ -328,7 +332,7 @@ def run_ours(args, rank, world, dist):
 
         def e2e_step():
             for i, (mid, mv, W, H) in enumerate(jobs):
-                r.render_into_host(mid, W, H, host[3 * offs[i]:3 * offs[i + 1]], mv=mv)
+                r.render_into_host(mid, W, H, host[3 * offs[i]:3 * offs[i + 1]], mv=mv, mode=mode)
     for _ in range(max(1, args.warmup)):
         e2e_step()
     t0 = time.perf_counter()
@@ -358,7 +362,7 @@ def run_ours(args, rank, world, dist):
                 "traffic": load_traffic(wl["name"]),
                 "algorithmic_bytes_per_launch": int(bytes_per_launch),
                 "bytes_per_step": BYTES_PER_STEP,
-                "kernel": "vfr::traverse_kernel<0,2>" + (" (one launch for all jobs)"
+                "kernel": f"vfr::traverse_kernel<{1 if args.mode == 'composited' else 0},2>" + (" (one launch for all jobs)"
                                                         if launches_per_trav == 1 else " (per job)"),
                 "launch_ms_mean": round(float(trav_ms.mean()), 4),
                 "gsteps_per_s": round(float(steps_step / launches_per_trav * len(trav_ms)
@@ -371,7 +375,8 @@ def run_ours(args, rank, world, dist):
     if rank != 0:
         return None
     out = {
-        "metric": f"Mrays/s ({wl['desc']})", "value": round(float(value), 2), "unit": "Mrays/s",
+        "metric": f"Mrays/s ({wl['desc']})" + (" [composited]" if args.mode == "composited" else ""),
+        "value": round(float(value), 2), "unit": "Mrays/s",
         "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": round(float(t_main / K), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded meshes, TF and views)",
@@ -380,7 +385,9 @@ def run_ours(args, rank, world, dist):
                                "verts": int(p["vert"].shape[0]),
                                "ext_faces": int(p["extf"].shape[0])} for p in wl["meshes"]],
                    "jobs": nj, "pixels_per_step": int(npix), "rays_per_step": rays_step,
-                   "tet_steps_per_step": steps_step, "mode": "reference (last visible face wins)",
+                   "tet_steps_per_step": steps_step,
+                   "mode": ("composited (every entry segment, depth-ordered)" if args.mode == "composited"
+                            else "reference (last visible face wins)"),
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "parallelism": f"{world} replica(s), one per GPU", "tuning": tuning},
         "fps": round(float(nj * world * K / (t_main * 1e-3)), 2),
@@ -589,6 +596,9 @@ def main():
     out, wl = res
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(wl, args.cpu_seconds)
+        if args.mode == "composited":
+            out["cpu_baseline"]["sample"] += (" (its own last-visible-face render: the reference "
+                                              "has no composited mode)")
     if dist:
         dist.destroy_process_group()
     print(_json(out))
