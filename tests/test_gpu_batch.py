@@ -89,3 +89,41 @@ def test_batch_outliving_its_context_is_safe():
     r.close()
     assert B.lib.vfr_batch_run(B.h) == vb._lib.VFR_ERR_STATE
     B.close()
+
+
+def test_batch_with_rayless_jobs(renderer):
+    """Jobs whose images no face covers (the single tet at 2x2 and 2x5) mixed
+    with jobs that have rays, and a batch of rayless jobs only: empty
+    segments of the ray queue, zero totals, images zeroed."""
+    from tests.conftest import load_golden
+
+    d = load_golden("single_tet")
+    renderer.upload_tables(d["tf"], d["psi"])
+    mid = renderer.upload_mesh(d["vert"], d["tet"], d["con"], d["extf"], d["lmt"])
+    try:
+        for jobs in ([(mid, None, 2, 2), (mid, None, 4, 4), (mid, None, 2, 5), (mid, None, 3, 3)],
+                     [(mid, None, 2, 2), (mid, None, 2, 5)]):
+            for graph in (False, True):
+                B = vbatch.BatchRenderer(renderer, jobs, graph=graph)
+                try:
+                    B.prepare()
+                    B.run()
+                    stats = B.stats()
+                    npx = sum(W * H for (_, _, W, H) in jobs)
+                    rgb = np.full(npx * 3, 77, np.uint8)
+                    steps = np.full(npx, 77, np.uint32)
+                    B.read(rgb8=rgb, steps=steps)
+                    off = 0
+                    for j, (m_, mv, W, H) in enumerate(jobs):
+                        single = renderer.render(m_, W, H)
+                        n = W * H
+                        assert stats[j]["num_rays"] == single["stats"]["num_rays"]
+                        assert np.array_equal(rgb[3 * off:3 * (off + n)].reshape(H, W, 3),
+                                              single["rgb8"])
+                        assert np.array_equal(steps[off:off + n].reshape(H, W), single["steps"])
+                        off += n
+                    assert [s["num_rays"] for s in stats][:1] == [0]
+                finally:
+                    B.close()
+    finally:
+        renderer.release_mesh(mid)

@@ -61,6 +61,18 @@ def test_rejects_unusable_max_edge(renderer, case):
                case["con"], case["extf"], lmt)
 
 
+def test_rejects_oversized_and_degenerate_images(renderer, case):
+    """More than 2^28 pixels, or a side below 2 (the reference divides by
+    res - 1), is refused before anything is allocated or launched."""
+    mid = renderer.upload_mesh(case["vert"], case["tet"], case["con"], case["extf"], case["lmt"])
+    try:
+        for W, H in ((1 << 15, 1 << 14), (1, 64), (64, 1), (0, 0)):
+            expect(vb._lib.VFR_ERR_INVALID, renderer.render_device, mid, W, H)
+        renderer.render(mid, 16, 16)  # the context is still usable
+    finally:
+        renderer.release_mesh(mid)
+
+
 def test_stage_order_and_handles(renderer, case):
     mid = renderer.upload_mesh(case["vert"], case["tet"], case["con"], case["extf"], case["lmt"])
     try:
