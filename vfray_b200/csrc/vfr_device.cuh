@@ -116,8 +116,9 @@ __device__ __forceinline__ void face_plane_ieee(float4 a, float4 b, float4 c, Pl
 // (div_by).  A coefficient of at least 2^-125 in magnitude is a quotient in
 // the normal range, so div_by gave it exactly.  When any coefficient is
 // smaller (zero included: rare, a face with an exactly constant depth or
-// scalar along an axis), the plane is solved again with IEEE divisions.
-__device__ __forceinline__ void face_plane(float4 a, float4 b, float4 c, Plane& p) {
+// scalar along an axis), this returns false and the plane must be solved
+// again with IEEE divisions (face_plane does so).
+__device__ __forceinline__ bool face_plane_fast(float4 a, float4 b, float4 c, Plane& p) {
   const float c0x = a.x, c0y = b.x, c0z = c.x;
   const float c1x = a.y, c1y = b.y, c1z = c.y;
   const float cross = fsub(fmul(c0y, c1z), fmul(c1y, c0z));
@@ -145,7 +146,11 @@ __device__ __forceinline__ void face_plane(float4 a, float4 b, float4 c, Plane& 
   }
   const float m = fminf(fminf(fminf(fabsf(p.zx), fabsf(p.zy)), fminf(fabsf(p.zz), fabsf(p.sx))),
                         fminf(fabsf(p.sy), fabsf(p.sz)));
-  if (!(m >= 0x1p-125f)) face_plane_ieee(a, b, c, p);
+  return m >= 0x1p-125f;
+}
+
+__device__ __forceinline__ void face_plane(float4 a, float4 b, float4 c, Plane& p) {
+  if (!face_plane_fast(a, b, c, p)) face_plane_ieee(a, b, c, p);
 }
 
 // a*x + b*y + c, left to right, no FMA
@@ -228,7 +233,9 @@ static __device__ __noinline__ int psi_coord_double(float tau) {
   return (int)min((uint32_t)fmul(tc, 512.0f), 511u);
 }
 
-__device__ __forceinline__ int psi_coord(float tau) {
+// The bracket alone: the coordinate (-1 to 511 whatever tau is, so it can
+// index the table), and in ok whether it is the reference's.
+__device__ __forceinline__ int psi_coord_fast(float tau, bool& ok) {
   // the bracket, computed for every tau (tau = 0 gives coordinate 0 here,
   // as gamma = 0 and tc = 2^-10 do in the reference); only its verdict
   // depends on the domain 0 <= tau < 2^20
@@ -238,8 +245,13 @@ __device__ __forceinline__ int psi_coord(float tau) {
   const float flo = __fmaf_rd(tlo, 512.0f, 0x1p23f);
   const float fhi = __fmaf_rd(thi, 512.0f, 0x1p23f);
   const bool out = tlo > 1.0f;
-  const bool ok = tau >= 0.0f && tau < 1048576.0f && (out || (thi <= 1.0f && flo == fhi));
-  int r = out ? -1 : (int)min(__float_as_uint(flo) - 0x4b000000u, 511u);
+  ok = tau >= 0.0f && tau < 1048576.0f && (out || (thi <= 1.0f && flo == fhi));
+  return out ? -1 : (int)min(__float_as_uint(flo) - 0x4b000000u, 511u);
+}
+
+__device__ __forceinline__ int psi_coord(float tau) {
+  bool ok;
+  int r = psi_coord_fast(tau, ok);
   if (!ok) r = psi_coord_double(tau);
   return r;
 }
@@ -256,8 +268,10 @@ __device__ __forceinline__ int psi_coord(float tau) {
 // then gives the reference's zeta unless the 29 bits that rounding drops
 // lie within 1024 units of the half-way pattern 2^28 (about one case in
 // 2^18): those cases, and x outside [-80, 0], take the double exp.
-// e2tab holds 2^(j/64), j = 0..63, rounded to double.
-__device__ __forceinline__ float zeta_of(double x, const double* e2tab) {
+// e2tab holds 2^(j/64), j = 0..63, rounded to double.  zeta_fast returns the
+// estimate rounded to float and, in ok, whether it is the reference's zeta;
+// zeta_of takes the double exp when it is not.
+__device__ __forceinline__ float zeta_fast(double x, const double* e2tab, bool& ok) {
   // computed for every x (e2tab is indexed in range whatever x is); only
   // the verdict depends on the domain -80 <= x <= 0
   const double kShift = 0x1.8p52;  // adding 1.5 * 2^52 rounds to an integer
@@ -274,8 +288,14 @@ __device__ __forceinline__ float zeta_of(double x, const double* e2tab) {
   // times 2^(k >> 6): the exponent field stays far above the subnormals
   e = __hiloint2double(__double2hiint(e) + (k >> 6) * (1 << 20), __double2loint(e));
   const uint32_t dropped = (uint32_t)__double2loint(e) & 0x1fffffffu;
-  float z = (float)e;
-  if (!(x >= -80.0 && x <= 0.0 && dropped - (0x10000000u - 1024u) > 2048u)) z = (float)exp(x);
+  ok = x >= -80.0 && x <= 0.0 && dropped - (0x10000000u - 1024u) > 2048u;
+  return (float)e;
+}
+
+__device__ __forceinline__ float zeta_of(double x, const double* e2tab) {
+  bool ok;
+  float z = zeta_fast(x, e2tab, ok);
+  if (!ok) z = (float)exp(x);
   return z;
 }
 

@@ -7,8 +7,9 @@
 // warp-aggregated atomicAdd), so lanes do not wait for the longest ray of
 // their warp.  The kernel is bound by instruction issue, so the step is
 // written to keep lanes converged: its arithmetic is branch-free, its rare
-// exact fallbacks (psi coordinate, exp, plane re-solve) sit out of line, and
-// every way a step can end is a status rather than an early return.  The current tet's 4 vertices live in
+// exact fallbacks (psi coordinate, exp, plane re-solve) are taken in one
+// block after the fast path, and every way a step can end is a status
+// rather than an early return.  The current tet's 4 vertices live in
 // registers rotated by the entry face f (r_j = local vertex (f + j) & 3), so
 // the three exit candidates (f+1, f+2, f+3) read fixed registers: candidate
 // i uses (r_i, r_i+1, r_i+2).  Once the exit face is known, a step issues its
@@ -166,11 +167,67 @@ __device__ __forceinline__ void finish_pixel(const JobDev& J, const Ray& R) {
 
 enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kAbandon = 2, kCap = 3, kRange = 4 };
 
+// The step's depth difference and extinctions from the exit face's depth zn
+// and scalar sn at the pixel (:437-457): dz = |zPrev - zNext| (0 below
+// RDELTA) / maxEdgeLength, the front's transfer-function entry, tau of the
+// front and of the back.  The step ends when sn is outside [0, 1] (:446).
+__device__ __forceinline__ void extinction(const SharedTables& S, const Ray& R, float zn, float sn,
+                                           uint32_t& st, uint32_t& tfi, float& taux,
+                                           float& tauy) {
+  float dz = fsub(R.zp, zn);
+  dz = dz < 0.0f ? -dz : dz;
+  dz = below_rdelta(dz) ? 0.0f : dz;
+  st = (st == kContinue && ((sn < 0.0f) || (sn > 1.0f))) ? kSegmentEnd : st;
+  // dz /= maxEdgeLength (:450): dz is 0 or at least 1e-12 and maxEdgeLength
+  // below 2^80 (checked at upload; view set-up gives at most 2 sqrt 3), so
+  // the quotient is never subnormal and div_by is exact
+  dz = div_by(dz, R.rmaxEdge);
+  tfi = min((uint32_t)fmul(255.0f, sn), 255u);  // colorFront (:452)
+  taux = fmul(S.a[tfi], dz);
+  tauy = fmul(S.a[R.cbi], dz);
+}
+
+// zeta's argument -(tau_f*0.5 + tau_b*0.5), in double (:459)
+__device__ __forceinline__ double zeta_arg(float taux, float tauy) {
+  return -dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5));
+}
+
+struct StepColour {
+  float r, g, b, t;
+};
+
+// The step's colour and transparency (:461-483) from the front's
+// transfer-function entry, zeta and the psi coordinates (any of -1..511:
+// the table is indexed in range whatever they are).
+__device__ __forceinline__ StepColour composite(const TraverseParams& P, const SharedTables& S,
+                                               const Ray& R, uint32_t tfi, float zeta, int ci,
+                                               int cj) {
+  const double psi = (double)__ldg(P.psi + (uint32_t)max(ci, 0) * 512u + (uint32_t)max(cj, 0));
+  const double dzeta = (double)zeta;
+  const double ca = dsub(1.0, psi), cbk = dsub(psi, dzeta);
+  const double2 frg = S.rg[tfi], brg = S.rg[R.cbi];
+  const double fbl = S.b[tfi], bbl = S.b[R.cbi];
+  const float fr = (float)dadd(dmul(frg.x, ca), dmul(brg.x, cbk));
+  const float fg = (float)dadd(dmul(frg.y, ca), dmul(brg.y, cbk));
+  const float fb = (float)dadd(dmul(fbl, ca), dmul(bbl, cbk));
+  const float fw = fsub(1.0f, zeta);           // (float)(1.0 - zeta), innocuous double rounding
+  const double keep = dsub(1.0, (double)fw);   // exact
+  StepColour o;
+  o.r = (float)dadd((double)fr, dmul(keep, (double)R.ar));
+  o.g = (float)dadd((double)fg, dmul(keep, (double)R.ag));
+  o.b = (float)dadd((double)fb, dmul(keep, (double)R.ab));
+  o.t = fmul(R.tr, zeta);
+  return o;
+}
+
 // One iteration of the reference's while loop (:302-542).  The ways it can
 // end before compositing (step cap, no exit face, id range, scalar or psi
 // coordinate out of range) are folded into a status and the arithmetic runs
-// on for every lane; the ray's state is only committed while the status
-// says to go on, so no lane takes an early branch.
+// on for every lane; the colour is only committed while the status says to
+// go on, so no lane takes an early branch.  The exact fallbacks of the
+// plane, zeta and the psi coordinates are gathered into one rare block
+// after the fast path, so the step from the exit tests to the advance is
+// one straight run of code that the compiler schedules as a whole.
 __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTables& S, Ray& R) {
   uint32_t st = (++R.iters > R.cap) ? kCap : kContinue;
   const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
@@ -194,53 +251,50 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   const float4 a = pick3(i, R.r1, R.r2, R.r3);
   const float4 b = pick3(i, R.r2, R.r3, R.r0);
   const float4 c = pick3(i, R.r3, R.r0, R.r1);
+  // fast path: every quantity from its branch-free estimate, with a flag
+  // where the estimate may differ from the reference's value
   Plane nf;
-  face_plane(a, b, c, nf);
-  const float zn = plane_eval(R.ox, R.oy, nf.zx, nf.zy, nf.zz);
-  const float sn = plane_eval(R.ox, R.oy, nf.sx, nf.sy, nf.sz);
-  float dz = fsub(R.zp, zn);
-  dz = dz < 0.0f ? -dz : dz;
-  dz = below_rdelta(dz) ? 0.0f : dz;
-  st = (st == kContinue && ((sn < 0.0f) || (sn > 1.0f))) ? kSegmentEnd : st;  // :446
-  // dz /= maxEdgeLength (:450): dz is 0 or at least 1e-12 and maxEdgeLength
-  // below 2^80 (checked at upload; view set-up gives at most 2 sqrt 3), so
-  // the quotient is never subnormal and div_by is exact
-  dz = div_by(dz, R.rmaxEdge);
-  const uint32_t tfi = min((uint32_t)fmul(255.0f, sn), 255u);  // colorFront (:452)
-  const float taux = fmul(S.a[tfi], dz), tauy = fmul(S.a[R.cbi], dz);
-  {
-    const float zeta = zeta_of(-dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5)), S.e2);
-    const int ci = psi_coord(taux), cj = psi_coord(tauy);
-    st = (st == kContinue && (ci | cj) < 0) ? kSegmentEnd : st;  // :468
-    const double psi = (double)__ldg(P.psi + (uint32_t)max(ci, 0) * 512u + (uint32_t)max(cj, 0));
-    const double dzeta = (double)zeta;
-    const double ca = dsub(1.0, psi), cbk = dsub(psi, dzeta);
-    const double2 frg = S.rg[tfi], brg = S.rg[R.cbi];
-    const double fbl = S.b[tfi], bbl = S.b[R.cbi];
-    const float fr = (float)dadd(dmul(frg.x, ca), dmul(brg.x, cbk));
-    const float fg = (float)dadd(dmul(frg.y, ca), dmul(brg.y, cbk));
-    const float fb = (float)dadd(dmul(fbl, ca), dmul(bbl, cbk));
-    const float fw = fsub(1.0f, zeta);           // (float)(1.0 - zeta), innocuous double rounding
-    const double keep = dsub(1.0, (double)fw);   // exact
-    const float ar = (float)dadd((double)fr, dmul(keep, (double)R.ar));
-    const float ag = (float)dadd((double)fg, dmul(keep, (double)R.ag));
-    const float ab = (float)dadd((double)fb, dmul(keep, (double)R.ab));
-    const float tr = fmul(R.tr, zeta);
-    if (st == kContinue) {
-      R.ar = ar;
-      R.ag = ag;
-      R.ab = ab;
-      R.tr = tr;
-      R.lastZ = zn;
-      R.cbi = tfi;
-      st = leaving ? kSegmentEnd : st;  // :535
+  const bool plane_ok = face_plane_fast(a, b, c, nf);
+  float zn = plane_eval(R.ox, R.oy, nf.zx, nf.zy, nf.zz);
+  const uint32_t st0 = st;
+  uint32_t tfi;
+  float taux, tauy;
+  extinction(S, R, zn, plane_eval(R.ox, R.oy, nf.sx, nf.sy, nf.sz), st, tfi, taux, tauy);
+  bool z_ok, i_ok, j_ok;
+  float zeta = zeta_fast(zeta_arg(taux, tauy), S.e2, z_ok);
+  int ci = psi_coord_fast(taux, i_ok), cj = psi_coord_fast(tauy, j_ok);
+  StepColour col = composite(P, S, R, tfi, zeta, ci, cj);
+  // rare: the exact path for the lanes whose plane, zeta or psi coordinate
+  // was not certified (a plane with a tiny coefficient; about one psi
+  // coordinate in 2^10), before anything is committed
+  if ((!plane_ok && st0 == kContinue) || (st == kContinue && !(z_ok && i_ok && j_ok))) {
+    if (!plane_ok) {
+      face_plane_ieee(a, b, c, nf);
+      zn = plane_eval(R.ox, R.oy, nf.zx, nf.zy, nf.zz);
+      st = st0;
+      extinction(S, R, zn, plane_eval(R.ox, R.oy, nf.sx, nf.sy, nf.sz), st, tfi, taux, tauy);
     }
+    zeta = zeta_of(zeta_arg(taux, tauy), S.e2);
+    ci = psi_coord(taux);
+    cj = psi_coord(tauy);
+    col = composite(P, S, R, tfi, zeta, ci, cj);
   }
-  if (st != kContinue) return st;
+  st = (st == kContinue && (ci | cj) < 0) ? kSegmentEnd : st;  // :468
+  if (st == kContinue) {
+    R.ar = col.r;
+    R.ag = col.g;
+    R.ab = col.b;
+    R.tr = col.t;
+    R.lastZ = zn;
+    R.cbi = tfi;
+    st = leaving ? kSegmentEnd : st;  // :535
+  }
   // advance to tn through its face fn: slots fn..fn+2 are the exit face's
-  // vertices in tn's order (permutation code), slot fn+3 is the loaded vertex
+  // vertices in tn's order (permutation code), slot fn+3 is the loaded
+  // vertex.  Done whatever the status: once a ray's segment ends, nothing
+  // reads its walk state before begin_segment sets it again.
   const uint32_t fn = (q >> 27) & 3u, code = q >> 29;
-  if (code < 6) {
+  {
     // per component two selects (a struct-wide select compiles to branches)
     const uint32_t pc = perm_code(code);
     const bool b0 = (pc & 3u) == 1u, c0 = (pc & 3u) == 2u;
@@ -255,7 +309,9 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
                        VFR_PICK(b2, c2, w));
 #undef VFR_PICK
     R.r3 = nv;
-  } else {  // shared face not matched by vertex ids: reload the tet's vertices
+  }
+  if (st == kContinue && code >= 6) {
+    // shared face not matched by vertex ids: reload the tet's vertices
     const uint4 id = __ldg(P.jobs[R.j].tet + tn);
     R.r0 = __ldg(R.vert + sel4(id, fn));
     R.r1 = __ldg(R.vert + sel4(id, (fn + 1) & 3u));
@@ -266,7 +322,7 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   R.t = tn;
   R.f = fn;
   R.zp = zn;
-  return kContinue;
+  return st;
 }
 
 // Per-lane tallies of tet-walk steps and status bits, flushed to the job's
