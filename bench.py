@@ -313,7 +313,8 @@ def run_ours(args, rank, world, dist):
     assert sum(x["num_rays"] for x in bst) == rays_step, "batched rays differ from single views"
     assert sum(x["num_steps"] for x in bst) == steps_step, "batched steps differ"
     kp = max(1, min(args.steps, 3))
-    t_plain, prof_plain = timed(plain_step, kp, 1, profile=True)
+    t_plain, _ = timed(plain_step, kp, 1)
+    prof_plain = timed(plain_step, 1, 0, profile=True)[1] if args.form == "plain" else None
     t_batch, _ = timed(batched_step, kp, 1)
     # stage times of the batched chain: the same batch launched directly
     # (not as a graph) with events between its stages
@@ -350,6 +351,9 @@ def run_ours(args, rank, world, dist):
     value, e2e = mrays(t_main, K), mrays(t_e2e, K)
 
     peak, peak_kind = load_peaks()
+    # traversal CTAs per SM the register budget allows: 2 + the tuned variant
+    # (without the autotuner, the library's default variant 1)
+    kmin = 2 + (tuning["variant"] if tuning else 1)
     trav_ms = prof[:, 2] if prof is not None and len(prof) else None
     roof = None
     if trav_ms is not None:
@@ -362,8 +366,8 @@ def run_ours(args, rank, world, dist):
                 "traffic": load_traffic(wl["name"]),
                 "algorithmic_bytes_per_launch": int(bytes_per_launch),
                 "bytes_per_step": BYTES_PER_STEP,
-                "kernel": f"vfr::traverse_kernel<{1 if args.mode == 'composited' else 0},2>" + (" (one launch for all jobs)"
-                                                        if launches_per_trav == 1 else " (per job)"),
+                "kernel": f"vfr::traverse_kernel<{1 if args.mode == 'composited' else 0},{kmin}>"
+                          + (" (one launch for all jobs)" if launches_per_trav == 1 else " (per job)"),
                 "launch_ms_mean": round(float(trav_ms.mean()), 4),
                 "gsteps_per_s": round(float(steps_step / launches_per_trav * len(trav_ms)
                                             / (trav_ms.sum() * 1e-3) / 1e9), 2),

@@ -53,10 +53,10 @@ extern "C" {
 #define VFR_OPT_QUEUE_CHUNK 2     /* rays a warp takes from the work queue at a time (32) */
 #define VFR_OPT_BLOCKS_PER_SM 3   /* traversal CTAs per SM; 0 = occupancy maximum */
 #define VFR_OPT_PROFILE 4         /* 1: record per-stage CUDA events of every view */
-#define VFR_OPT_TRAVERSE_VARIANT 5 /* traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM */
+#define VFR_OPT_TRAVERSE_VARIANT 5 /* traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM (1) */
 #define VFR_OPT_REFILL 6          /* refill a warp's idle lanes once >= this many are idle (4) */
 #define VFR_OPT_RASTER_WARPS 7    /* stage (b) warps per SM (64) */
-#define VFR_OPT_TILE_WIDTH 8      /* ray-list screen tile width: 4, 8, 16, 32 (8 = 8x4) */
+#define VFR_OPT_TILE_WIDTH 8      /* ray-list screen tile width: 4, 8, 16, 32 (4 = 4x8) */
 
 /* Render modes. */
 #define VFR_MODE_REF 0        /* reference semantics: last visible face wins each pixel */

@@ -53,9 +53,9 @@ struct Mesh {
 struct Tuning {
   uint32_t blocks_per_sm = 0;  // traversal CTAs per SM (0: occupancy maximum)
   uint32_t refill = 4;         // refill idle lanes once this many of a warp's are idle
-  uint32_t variant = 0;        // traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM
+  uint32_t variant = 1;        // traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM
   uint32_t raster_warps_per_sm = 64;
-  uint32_t tile_w = 8;          // ray-list tile width (x 32/tile_w rows)
+  uint32_t tile_w = 4;          // ray-list tile width (x 32/tile_w rows)
 };
 
 struct Ctx;
