@@ -7,7 +7,10 @@ it accepts.
   s, cr with cr >= 0x2b8cbccd  <=>  float(s - cr) <= 0x2b8cbccc;
 * psi coordinate (:462-471): the float bracket around gamma = tau/(1.0+tau)
   selects the reference's table coordinate whenever its two ends agree, for
-  any quotient estimate within the 2-ulp bound of __fdividef.
+  any quotient estimate within the 2-ulp bound of __fdividef;
+* keep = 1 - a of the compositing (:474-483) as zeta rounded to the 2^-24
+  grid, for zeta in [0, 1];
+* zeta's argument (:459) as one halved double sum.
 """
 import numpy as np
 
@@ -113,3 +116,46 @@ def test_division_through_a_shared_reciprocal():
         normal = np.abs(want) >= F32(2.0 ** -126)
         assert normal.mean() > 0.9
         assert np.array_equal(got[normal], want[normal])
+
+
+def test_keep_is_zeta_on_the_2_pow_minus_24_grid():
+    """keep = 1.0 - (double)(float)(1.0 - zeta) (:474-483) for a float zeta in
+    [0, 1] is zeta rounded to a multiple of 2^-24, ties to even, which the
+    kernel's fast path computes as (zeta + 1.5 * 2^28) - 1.5 * 2^28 in double.
+    Checked on every float in [2^-27, 1] and on zero."""
+    C = np.float64(1.5 * 2.0 ** 28)
+    one = F32(1.0)
+    for e in range(-27, 0):  # binade [2^e, 2^(e+1))
+        lo = np.array([2.0 ** e], F32).view(np.uint32)[0]
+        hi = np.array([2.0 ** (e + 1)], F32).view(np.uint32)[0]
+        z = np.arange(lo, hi, dtype=np.uint32).view(F32)
+        ref = 1.0 - (one - z).astype(np.float64)
+        new = (z.astype(np.float64) + C) - C
+        assert np.array_equal(ref.view(np.uint64), new.view(np.uint64)), e
+    for z in (F32(0.0), F32(1.0), F32(2.0 ** -28), F32(1e-30)):
+        z = np.array([z], F32)
+        ref = 1.0 - (one - z).astype(np.float64)
+        new = (z.astype(np.float64) + C) - C
+        assert ref[0] == new[0]
+
+
+def test_zeta_argument_as_one_halved_sum():
+    """-(tau_f*0.5 + tau_b*0.5) in double (:459) equals (tau_f + tau_b) * -0.5
+    for any floats: halving is exact and commutes with rounding, as no double
+    sum of two floats is subnormal.  Bit for bit, signed zeros and infinities
+    included."""
+    rng = np.random.default_rng(11)
+    for _ in range(4):
+        n = 2_000_000
+        a = (rng.uniform(0.5, 1.0, n) * 2.0 ** rng.integers(-149, 128, n)).astype(F32)
+        b = (rng.uniform(0.5, 1.0, n) * 2.0 ** rng.integers(-149, 128, n)).astype(F32)
+        near = rng.random(n) < 0.5  # half the pairs within a few binades of each other
+        with np.errstate(over="ignore"):  # a few overflow to infinity, which stays exact
+            b[near] = (a[near].astype(np.float64) * rng.uniform(0.01, 100, near.sum())).astype(F32)
+        b[rng.random(n) < 0.01] = 0.0
+        a64, b64 = a.astype(np.float64), b.astype(np.float64)
+        ref = -((a64 * 0.5) + (b64 * 0.5))
+        new = (a64 + b64) * -0.5
+        assert np.array_equal(ref.view(np.uint64), new.view(np.uint64))
+    z = np.zeros(1)
+    assert (-((z * 0.5) + (z * 0.5))).view(np.uint64)[0] == ((z + z) * -0.5).view(np.uint64)[0]

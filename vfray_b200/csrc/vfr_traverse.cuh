@@ -187,9 +187,11 @@ __device__ __forceinline__ void extinction(const SharedTables& S, const Ray& R, 
   tauy = fmul(S.a[R.cbi], dz);
 }
 
-// zeta's argument -(tau_f*0.5 + tau_b*0.5), in double (:459)
+// zeta's argument -(tau_f*0.5 + tau_b*0.5), in double (:459).  Halving is
+// exact and commutes with rounding (a double sum of two floats is never
+// subnormal), so it is the sum times -0.5: one multiplication fewer.
 __device__ __forceinline__ double zeta_arg(float taux, float tauy) {
-  return -dadd(dmul((double)taux, 0.5), dmul((double)tauy, 0.5));
+  return dmul(dadd((double)taux, (double)tauy), -0.5);
 }
 
 struct StepColour {
@@ -198,7 +200,10 @@ struct StepColour {
 
 // The step's colour and transparency (:461-483) from the front's
 // transfer-function entry, zeta and the psi coordinates (any of -1..511:
-// the table is indexed in range whatever they are).
+// the table is indexed in range whatever they are).  kUnitZeta: zeta is
+// known to lie in [0, 1] (the fast path's certified zeta), which lets
+// 1 - a be formed without a conversion.
+template <bool kUnitZeta>
 __device__ __forceinline__ StepColour composite(const TraverseParams& P, const SharedTables& S,
                                                const Ray& R, uint32_t tfi, float zeta, int ci,
                                                int cj) {
@@ -210,8 +215,19 @@ __device__ __forceinline__ StepColour composite(const TraverseParams& P, const S
   const float fr = (float)dadd(dmul(frg.x, ca), dmul(brg.x, cbk));
   const float fg = (float)dadd(dmul(frg.y, ca), dmul(brg.y, cbk));
   const float fb = (float)dadd(dmul(fbl, ca), dmul(bbl, cbk));
-  const float fw = fsub(1.0f, zeta);           // (float)(1.0 - zeta), innocuous double rounding
-  const double keep = dsub(1.0, (double)fw);   // exact
+  // keep = 1 - a with a = (float)(1.0 - zeta) (innocuous double rounding);
+  // 1 - a is exact.  For zeta in [0, 1], a is 1 - zeta exactly when
+  // zeta >= 0.5 and otherwise 1 - zeta rounded to the 2^-24 grid of the
+  // floats in [0.5, 1]; either way 1 - a is zeta rounded to a multiple of
+  // 2^-24, ties to even, which adding and removing 1.5 * 2^28 in double
+  // gives.
+  double keep;
+  if (kUnitZeta) {
+    keep = dsub(dadd(dzeta, 0x1.8p28), 0x1.8p28);
+  } else {
+    const float fw = fsub(1.0f, zeta);
+    keep = dsub(1.0, (double)fw);
+  }
   StepColour o;
   o.r = (float)dadd((double)fr, dmul(keep, (double)R.ar));
   o.g = (float)dadd((double)fg, dmul(keep, (double)R.ag));
@@ -263,7 +279,7 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   bool z_ok, i_ok, j_ok;
   float zeta = zeta_fast(zeta_arg(taux, tauy), S.e2, z_ok);
   int ci = psi_coord_fast(taux, i_ok), cj = psi_coord_fast(tauy, j_ok);
-  StepColour col = composite(P, S, R, tfi, zeta, ci, cj);
+  StepColour col = composite<true>(P, S, R, tfi, zeta, ci, cj);
   // rare: the exact path for the lanes whose plane, zeta or psi coordinate
   // was not certified (a plane with a tiny coefficient; about one psi
   // coordinate in 2^10), before anything is committed
@@ -277,7 +293,7 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
     zeta = zeta_of(zeta_arg(taux, tauy), S.e2);
     ci = psi_coord(taux);
     cj = psi_coord(tauy);
-    col = composite(P, S, R, tfi, zeta, ci, cj);
+    col = composite<false>(P, S, R, tfi, zeta, ci, cj);
   }
   st = (st == kContinue && (ci | cj) < 0) ? kSegmentEnd : st;  // :468
   if (st == kContinue) {
