@@ -49,7 +49,13 @@ class Server:
         """(image, info) of a request; raises VfrError on its status."""
         info = RequestInfo()
         rc = self.lib.vfr_server_wait(self.h, ticket, timeout_ms, C.byref(info))
-        out = self._outs.pop(ticket, None)
+        # after a timeout the request is still in flight and the server will
+        # write its image later: its buffer stays referenced until a wait
+        # that returns the request's own status
+        if rc == _lib.VFR_ERR_TIMEOUT:
+            out = self._outs.get(ticket)
+        else:
+            out = self._outs.pop(ticket, None)
         check(rc, None, "vfr_server_wait")
         return out, info.as_dict()
 
