@@ -1,9 +1,13 @@
-"""Host logic of the served form's Python wrapper, without a GPU: the image
-buffer of a request must stay referenced while the request is in flight.
-vfr_server_wait returns VFR_ERR_TIMEOUT while the request is still queued or
-rendering (the server writes its image later), and the request's own status
-once it is done and forgotten.  The C server is replaced by a fake whose
-wait answers are scripted."""
+"""Buffer lifetimes in the Python wrappers of the served and batched forms,
+without a GPU.
+
+* Server: the image buffer of a request must stay referenced while the
+  request is in flight.  vfr_server_wait returns VFR_ERR_TIMEOUT while the
+  request is still queued or rendering (the server writes its image later),
+  and the request's own status once it is done and forgotten.  The C server
+  is replaced by a fake whose wait answers are scripted.
+* Batch jobs: the output tensors whose addresses a job records stay alive as
+  long as the job."""
 import gc
 import weakref
 
@@ -54,3 +58,22 @@ def test_buffer_released_with_the_request_status():
     with pytest.raises(_lib.VfrError) as e:
         s.wait(3)
     assert e.value.status == _lib.VFR_ERR_BUDGET and 3 not in s._outs
+
+
+def test_batch_job_keeps_its_output_tensors():
+    """A batch job records raw device addresses of its outputs (a captured
+    graph writes through them on every run); the job holds the tensors so
+    that a caller's temporaries are not freed under it."""
+    torch = pytest.importorskip("torch")
+    from vfray_b200.batch import job
+
+    t = torch.empty(2 * 2 * 3, dtype=torch.uint8)
+    ref = weakref.ref(t)
+    j = job(0, 2, 2, rgb8=t)
+    assert j.rgb8_dev == t.data_ptr()
+    del t
+    gc.collect()
+    assert ref() is not None
+    del j
+    gc.collect()
+    assert ref() is None

@@ -16,7 +16,10 @@ __all__ = ["BatchRenderer", "job"]
 
 def job(mesh_id: int, W: int, H: int, mv=None, rgb8=None, rgba=None, steps=None) -> Job:
     """A vfr_job; outputs are device buffers (torch CUDA tensors) or None
-    (then the batch owns its outputs when all three are None)."""
+    (then the batch owns its outputs when all three are None).  The job
+    holds references to its output tensors, and a BatchRenderer holds its
+    jobs, so the buffers outlive every launch (and captured graph) that
+    writes them."""
     j = Job()
     j.mesh_id = mesh_id
     j.W = W
@@ -29,6 +32,7 @@ def job(mesh_id: int, W: int, H: int, mv=None, rgb8=None, rgba=None, steps=None)
     j.rgb8_dev = None if rgb8 is None else rgb8.data_ptr()
     j.rgba_dev = None if rgba is None else rgba.data_ptr()
     j.steps_dev = None if steps is None else steps.data_ptr()
+    j._keep = tuple(t for t in (rgb8, rgba, steps) if t is not None)
     return j
 
 
@@ -49,7 +53,7 @@ class BatchRenderer:
 
     def set_jobs(self, jobs):
         js = [j if isinstance(j, Job) else job(j[0], j[2], j[3], mv=j[1]) for j in jobs]
-        self.jobs = js
+        self.jobs = js  # keeps each job's output tensors alive (job())
         arr = (Job * len(js))(*js)
         self._arr = arr
         check(self.lib.vfr_batch_set_jobs(self.h, arr, len(js), self.mode), self.r.h,
