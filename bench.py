@@ -10,26 +10,38 @@ Workloads (seeded synthetic meshes, transfer function and cameras):
   mixed    8 carved meshes with 16..128 cells per side and 256 jobs, each a
            random mesh, resolution in {128^2, 256^2, 512^2, 1024^2} and
            rotation; one step renders the 256 jobs.
-  served   the mixed meshes behind the request loop: Poisson arrivals at
-           several rates, requests at {256^2, 512^2, 1024^2}; p50/p99 latency
+  served   resident carved meshes behind the request loop: Poisson arrivals at
+           several rates, requests of several resolutions; p50/p99 latency
            and Mrays/s per rate.
   convex24 one 512x512 view of the convex 24^3 mesh.
   large    one 2048x2048 view of the carved 256^3 mesh (100.7 M tets before
            carving, 85.6 M after: 4.1 GB of tet and walk records, far beyond
            L2); building the mesh on the host takes about two minutes.
+Every workload renders with the reference's own psi table
+(psiGammaTable512.h, shipped with the library).
 
 Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events
 on the render stream after an L2 flush (a 256 MiB write) that is not timed;
 the step times are summed, the max over ranks is taken (N > 1 runs N
 replicas, one per GPU, weak scaling), and ``value`` = rays rendered by all
 ranks / that time.  A ray is a pixel with an entry face.  ``e2e`` is the same
-metric through the host-buffer API (camera in, RGB8 images out through pinned
-host memory, the copies inside the timed region).  ``roofline`` divides the
-traversal kernel's algorithmic bytes (48 B per tet-walk step: one 32-byte walk
-record + one new 16-byte vertex) by its event-timed launch duration.
-``cpu_baseline`` times the reference's own CPU kernels (built from the
-reference sources into oracle/_ref, -O3 -ffast-math as the reference builds
-them) on all host cores over a bounded sample of the same jobs.
+metric through the host-buffer API: every step copies the step's cameras from
+pinned host memory to the device and the RGB8 images back to pinned host
+memory, inside the timed region.  ``roofline`` divides the traversal kernel's
+algorithmic bytes (48 B per tet-walk step: one 32-byte walk record + one new
+16-byte vertex) by its event-timed launch duration.  ``cpu_baseline`` times
+the reference's own CPU kernels (built from the reference sources into
+oracle/_ref, -O3 -ffast-math as the reference builds them) on this host over
+a bounded sample of the same jobs: single-threaded as the reference is
+written, and on all host cores.
+
+``--impl reference`` times the reference's CPU path alone, in a process that
+loads none of this repository's product code: the workload's meshes are
+generated here, their adjacency computed by the oracle's numpy restatement,
+written as the reference's .off/.con/.extf/.tf files and read back through the
+reference's own readers; each step then renders every job of the workload
+with the reference's per-view sequence (rotateVolume, normalizeVertices,
+buildLmt, its three stages) on all host cores.
 """
 from __future__ import annotations
 
@@ -38,6 +50,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -47,6 +60,7 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_STEP = 48        # 32-byte walk record + one new 16-byte vertex
 FLUSH_BYTES = 256 << 20    # > 126 MB L2
+L2_NOTE = "GPU: flushed between timed steps (256 MiB write, untimed); CPU: not applicable"
 
 
 def parse():
@@ -63,8 +77,10 @@ def parse():
                     help="ref: the reference's last-visible-face image; composited: every "
                          "entry segment of each ray, depth-ordered")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="bound of the CPU-baseline sample")
+    ap.add_argument("--ref-step-seconds", type=float, default=60.0,
+                    help="reference arm: a step stops taking new jobs after this long")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rates", default="50,200,1000,2000", help="served: arrival rates (req/s)")
     ap.add_argument("--served-seconds", type=float, default=2.0)
@@ -76,44 +92,34 @@ def parse():
 MIXED_N = (16, 24, 32, 48, 64, 80, 96, 128)
 
 
-def _mesh(n, carved, seed_offset=0):
-    import vfray_b200 as vb
-    from vfray_b200 import synth
+def workload_spec(name, views=64):
+    """The workload as seeded inputs, numpy only: raw meshes (vertices not yet
+    normalised, tets), jobs (mesh index, model-view or None, W, H), the
+    transfer function and a description."""
+    from vfray_b200 import synth  # numpy only: loads no native library
 
-    vert, tet = synth.make_mesh(n, carved=carved, view_seed=None, jitter_seed=0 + seed_offset,
-                                scalar_seed=1 + seed_offset, carve_seed=4 + seed_offset)
-    p = vb.prepare(vert, tet)
-    p["n"] = n
-    return p
+    def carved(n, k=0):
+        v, t = synth.make_mesh(n, carved=True, view_seed=None, jitter_seed=0 + k,
+                               scalar_seed=1 + k, carve_seed=4 + k)
+        return dict(n=n, vert=v, tet=t)
 
-
-def make_workload(name, views=64):
-    """Meshes (prepared as vfRayPreComp would) and jobs (mesh index, model-view
-    or None, W, H)."""
-    import vfray_b200 as vb
-    from vfray_b200 import synth
-
-    wl = dict(name=name, tf=synth.transfer_function(2), psi=vb.psi_table())
+    sp = dict(name=name, tf=synth.transfer_function(2))
     if name == "orbit64":
-        wl["meshes"] = [_mesh(64, True)]
-        wl["jobs"] = [(0, mv, 512, 512) for mv in synth.orbit_views(views, seed=3)]
-        wl["desc"] = f"{views} orbit views at 512x512 of the carved 64^3 Freudenthal mesh"
+        sp["meshes"] = [carved(64)]
+        sp["jobs"] = [(0, mv, 512, 512) for mv in synth.orbit_views(views, seed=3)]
+        sp["desc"] = f"{views} orbit views at 512x512 of the carved 64^3 Freudenthal mesh"
     elif name == "large":
-        vert, tet = synth.make_mesh(256, carved=True, view_seed=3)
-        p = vb.prepare(vert, tet)
-        p["n"] = 256
-        wl["meshes"] = [p]
-        wl["jobs"] = [(0, None, 2048, 2048)]
-        wl["desc"] = "one 2048x2048 view of the carved 256^3 Freudenthal mesh (seeded rotation)"
+        v, t = synth.make_mesh(256, carved=True, view_seed=3)
+        sp["meshes"] = [dict(n=256, vert=v, tet=t)]
+        sp["jobs"] = [(0, None, 2048, 2048)]
+        sp["desc"] = "one 2048x2048 view of the carved 256^3 Freudenthal mesh (seeded rotation)"
     elif name == "convex24":
-        vert, tet = synth.make_mesh(24, carved=False, view_seed=3)
-        p = vb.prepare(vert, tet)
-        p["n"] = 24
-        wl["meshes"] = [p]
-        wl["jobs"] = [(0, None, 512, 512)]
-        wl["desc"] = "one 512x512 view of the convex 24^3 Freudenthal mesh (seeded rotation)"
-    else:  # mixed / served
-        wl["meshes"] = [_mesh(n, True, seed_offset=k) for k, n in enumerate(MIXED_N)]
+        v, t = synth.make_mesh(24, carved=False, view_seed=3)
+        sp["meshes"] = [dict(n=24, vert=v, tet=t)]
+        sp["jobs"] = [(0, None, 512, 512)]
+        sp["desc"] = "one 512x512 view of the convex 24^3 Freudenthal mesh (seeded rotation)"
+    else:  # mixed
+        sp["meshes"] = [carved(n, k) for k, n in enumerate(MIXED_N)]
         rng = np.random.default_rng(5)
         res = (128, 256, 512, 1024)
         jobs = []
@@ -124,10 +130,40 @@ def make_workload(name, views=64):
             mv = np.eye(4, dtype=np.float32)
             mv[:3, :3] = q * np.sign(np.linalg.det(q))
             jobs.append((m, mv, r, r))
-        wl["jobs"] = jobs
-        wl["desc"] = ("256 jobs over 8 carved meshes (16..128 cells per side), resolutions "
+        sp["jobs"] = jobs
+        sp["desc"] = ("256 jobs over 8 carved meshes (16..128 cells per side), resolutions "
                       "128^2..1024^2, random rotations")
-    return wl
+    return sp
+
+
+def prepare_ours(sp):
+    """The load sequence of the reference driver (normalizeVertices,
+    buildCon, buildExtF, buildLmt) through this library, and its default psi
+    table (the reference's own)."""
+    import vfray_b200 as vb
+
+    meshes = []
+    for m in sp["meshes"]:
+        p = vb.prepare(m["vert"], m["tet"])
+        p["n"] = m["n"]
+        meshes.append(p)
+    return dict(sp, meshes=meshes, psi=vb.reference_psi_table())
+
+
+def mesh_info(meshes):
+    return [{"cells": p["n"], "tets": int(p["tet"].shape[0]), "verts": int(p["vert"].shape[0]),
+             "ext_faces": int(p["extf"].shape[0])} for p in meshes]
+
+
+def workload_config(wl, rays_per_step, mode):
+    """The config both arms report: what the workload is, nothing about how
+    an arm runs it."""
+    return {"workload": wl["name"], "desc": wl["desc"], "meshes": mesh_info(wl["meshes"]),
+            "jobs": len(wl["jobs"]), "pixels_per_step": int(sum(W * H for (_, _, W, H) in wl["jobs"])),
+            "rays_per_step": int(rays_per_step),
+            "mode": ("composited (every entry segment, depth-ordered)" if mode == "composited"
+                     else "reference (last visible face wins)"),
+            "psi_table": "the reference's psiGammaTable512.h", "l2": L2_NOTE}
 
 
 def max_over_ranks(values, dist, device):
@@ -168,13 +204,26 @@ def load_traffic(name):
     return None
 
 
+def host_info():
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "cpu_model": model}
+
+
 class Clocks:
     """nvidia-smi sampled during the timed region."""
 
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join("/tmp", f"vfr_clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"vfr_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -221,6 +270,225 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+# ------------------------------------------------------------------ reference (CPU)
+
+class RefRunner:
+    """The reference's CPU path (oracle/_ref/libvfref_fast.so: its own
+    kernels and precomputation, -O3 -ffast-math as it builds them) over the
+    jobs of a workload.  ``meshes``: per mesh the normalised vertices, tets,
+    conTet, boundary count, external faces and limits as the reference holds
+    them.  A job is its driver's view change -- rotateVolume,
+    normalizeVertices and buildLmt of the new view (vfRay.cu:618-641,
+    vfRayPreComp.cc:84-145,808-853,886-906) -- then its three stages, on
+    ``threads`` host threads (1: the reference's own sequential loop)."""
+
+    def __init__(self, meshes, jobs, tf):
+        import oracle
+
+        self.R = oracle.Reference("fast")
+        self.R.set_tf(tf)
+        self.meshes, self.jobs, self.tf = meshes, jobs, tf
+        self.cur = None
+        self.rays_of = {}
+        self.S = None  # the strict build, for ray counts
+
+    def _load(self, m):
+        p = self.meshes[m]
+        if self.cur != m:
+            self.R.set_mesh(p["vert"], p["tet"])
+            self.R.set_con(p["con"], p["n_ext"])
+            self.R.set_extf(p["extf"])
+            self.cur = m
+        else:
+            self.R.set_vert(p["vert"])
+
+    def view(self, k):
+        m, mv, W, H = self.jobs[k]
+        self._load(m)
+        if mv is not None:
+            self.R.rotate(mv)
+            self.R.normalize()
+            self.R.build_lmt()
+        else:
+            self.R.set_lmt(*self.meshes[m]["lmt"])
+        return W, H
+
+    def job(self, k, threads):
+        W, H = self.view(k)
+        if threads == 1:
+            self.R.render(W, H, detect=False)
+        else:
+            self.R.render_mt(W, H, threads=threads)
+
+    def rays(self, k):
+        """Pixels with an entry face in job k (not timed): the oracle's
+        winner pass over the view as the reference's IEEE build sets it up
+        (normalizeVertices of the mesh, then per view rotateVolume +
+        normalizeVertices), the workload's own ray count.  The fast-math
+        build's set-up moves a handful of pixels in ten million across an
+        edge; the count does not follow it."""
+        if k not in self.rays_of:
+            import oracle
+
+            if self.S is None:
+                self.S = oracle.Reference("strict")
+            m, mv, W, H = self.jobs[k]
+            p = self.meshes[m]
+            self.S.set_mesh(p.get("vert_ieee", p["vert"]), p["tet"])
+            lmt = p["lmt"]
+            if mv is not None:
+                self.S.rotate(mv)
+                self.S.normalize()
+                self.S.build_lmt()
+                lmt = self.S.lmt()
+            Or = oracle.Oracle()
+            om = Or.mesh(self.S.vert(), p["tet"], p["con"], p["extf"], self.tf,
+                         np.zeros((512, 512), np.float32), lmt[0])
+            self.rays_of[k] = int((Or.winners(om, W, H) >= 0).sum())
+        return self.rays_of[k]
+
+
+def reference_meshes_from_files(sp, tmpdir):
+    """Each mesh of the workload as the reference's driver meets it: written
+    as .off/.con/.extf/.tf (adjacency from the oracle's numpy restatement of
+    buildIncid + buildCon), read back by the reference's readers
+    (vfRayPreComp.cc:29-69,375-420,551-590), normalised by its
+    normalizeVertices, limits from its buildLmt.  Meshes above 16 M tets are
+    handed over as arrays through the same state instead of text files
+    (parsing gigabytes of text is not the path being timed)."""
+    import oracle
+    from oracle import precomp
+
+    out = []
+    R = oracle.Reference("fast")
+    S = oracle.Reference("strict")
+    for i, m in enumerate(sp["meshes"]):
+        con, n_ext = precomp.build_con(m["tet"])
+        extf = precomp.build_extf(con)
+        if m["tet"].shape[0] <= (16 << 20):
+            base = os.path.join(tmpdir, f"mesh{i}")
+            precomp.write_off(base + ".off", m["vert"], m["tet"])
+            precomp.write_con(base + ".con", con, n_ext)
+            precomp.write_extf(base + ".extf", extf)
+            precomp.write_tf(base + ".tf", sp["tf"])
+            R.read_off(base + ".off")
+            R.read_con(base + ".con")
+            R.read_extf(base + ".extf")
+            R.read_tf(base + ".tf")
+            inputs = "files"
+        else:
+            R.set_mesh(m["vert"], m["tet"])
+            R.set_con(con, n_ext)
+            R.set_extf(extf)
+            R.set_tf(sp["tf"])
+            inputs = "arrays"
+        S.set_mesh(R.vert(), m["tet"])  # as read, before normalisation
+        S.normalize()
+        R.normalize()
+        R.build_lmt()
+        rc, rn = R.con()
+        out.append(dict(n=m["n"], vert=R.vert(), vert_ieee=S.vert(), tet=m["tet"], con=rc,
+                        n_ext=rn, extf=R.extf(), lmt=R.lmt(), tf=R.tf(), inputs=inputs))
+    return out
+
+
+def cpu_baseline(wl, seconds):
+    """The reference's CPU kernels on this host over a bounded sample of the
+    workload's jobs (in order): a third of the time single-threaded, as the
+    reference is written, the rest on all host cores."""
+    meshes = [dict(p, n_ext=int(p["extf"].shape[0])) for p in wl["meshes"]]
+    run = RefRunner(meshes, wl["jobs"], wl["tf"])
+    nthreads = os.cpu_count() or 1
+    legs = {}
+    for threads, budget in ((1, seconds / 3), (nthreads, 2 * seconds / 3)):
+        done, t, k = 0, 0.0, 0
+        rays = 0
+        while True:
+            t0 = time.perf_counter()
+            run.job(k, threads)
+            t += time.perf_counter() - t0
+            rays += run.rays(k)
+            done += 1
+            k = (k + 1) % len(wl["jobs"])
+            if t >= budget:
+                break
+        legs[threads] = (rays / t / 1e6, done, t)
+    v, done, t = legs[nthreads]
+    v1, done1, t1 = legs[1]
+    return dict({"value": round(v, 4), "unit": "Mrays/s", "cores": nthreads, "kind": "reference",
+                 "sample": f"{done} of {len(wl['jobs'])} jobs, reference vfRayKernelCPU.cc "
+                           f"(-O3 -ffast-math) on {nthreads} threads (column strips), {t:.1f} s, "
+                           "per job rotateVolume + normalizeVertices + buildLmt + the three stages",
+                 "single_thread": {"value": round(v1, 4), "unit": "Mrays/s", "cores": 1,
+                                   "sample": f"{done1} job(s), the reference's own sequential "
+                                             f"loop (main.cc:73-224), {t1:.1f} s"}},
+                **host_info())
+
+
+def product_library_loaded():
+    try:
+        with open("/proc/self/maps") as f:
+            return any("libvfray_b200" in line for line in f)
+    except OSError:
+        return None
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    import oracle
+
+    if not oracle.ref_available("fast"):
+        return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}
+    name = "mixed" if args.workload == "served" else args.workload
+    sp = workload_spec(name, args.views)
+    with tempfile.TemporaryDirectory() as tmp:
+        meshes = reference_meshes_from_files(sp, tmp)
+    wl = dict(sp, meshes=meshes)
+    run = RefRunner(meshes, sp["jobs"], meshes[0]["tf"])
+    nthreads = os.cpu_count() or 1
+    nj = len(sp["jobs"])
+    for w in range(args.warmup):  # the CPU needs no warm-up beyond one job
+        run.job(w % nj, nthreads)
+    total_t, rendered, full_steps = 0.0, [], 0
+    for _ in range(args.steps):
+        t_step, k = 0.0, 0
+        while k < nj:
+            t0 = time.perf_counter()
+            run.job(k, nthreads)
+            t_step += time.perf_counter() - t0
+            rendered.append(k)
+            k += 1
+            if t_step >= args.ref_step_seconds:
+                break
+        full_steps += k == nj
+        total_t += t_step
+    rays = sum(run.rays(k) for k in rendered)
+    v = rays / total_t / 1e6
+    rays_per_step = sum(run.rays(k) for k in range(nj)) if full_steps == args.steps else rays / args.steps
+    loaded = product_library_loaded()
+    return {"impl": "reference", "metric": f"Mrays/s ({sp['desc']})", "value": round(v, 4),
+            "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total_t / args.steps * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded meshes, TF and views)",
+            "config": workload_config(wl, rays_per_step, args.mode),
+            "steps_detail": {"jobs_per_step": len(rendered) / args.steps,
+                             "every_step_rendered_all_jobs": full_steps == args.steps,
+                             "warmup": "one job per warm-up step",
+                             "inputs": sorted({m["inputs"] for m in meshes}),
+                             "product_library_loaded": loaded},
+            "cpu_baseline": dict({"value": round(v, 4), "unit": "Mrays/s", "cores": nthreads,
+                                  "kind": "reference",
+                                  "sample": f"{len(rendered)} jobs over {args.steps} steps, "
+                                            "reference vfRayKernelCPU.cc (-O3 -ffast-math) on "
+                                            f"{nthreads} threads (column strips), per job "
+                                            "rotateVolume + normalizeVertices + buildLmt + the "
+                                            "three stages"}, **host_info()),
+            "e2e": {"value": round(v, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
 # ------------------------------------------------------------------ ours
 
 def setup_gpu(wl, dev):
@@ -244,7 +512,7 @@ def run_ours(args, rank, world, dist):
     from vfray_b200 import batch as vbatch
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
-    wl = make_workload(args.workload, args.views)
+    wl = prepare_ours(workload_spec(args.workload, args.views))
     r, stream, mids = setup_gpu(wl, dev)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     jobs = [(mids[m], mv, W, H) for (m, mv, W, H) in wl["jobs"]]
@@ -323,17 +591,23 @@ def run_ours(args, rank, world, dist):
     runner_p.close()
     prof, launches_per_trav = (prof_batch, 1) if args.form == "batched" else (prof_plain, nj)
 
-    # e2e through the host API: cameras in, RGB8 out through pinned memory
+    # e2e through the host API: every step, cameras in from pinned memory,
+    # the three stages, RGB8 out to pinned memory
     pinned = torch.empty(npix * 3, dtype=torch.uint8, pin_memory=True)
+    cams = torch.empty((nj, 4, 4), dtype=torch.float32, pin_memory=True)
+    for i, (_, mv, _, _) in enumerate(jobs):
+        cams[i] = torch.from_numpy(np.asarray(mv if mv is not None else np.eye(4), np.float32))
     if args.form == "batched":
         def e2e_step():
-            runner.run_host(pinned)
+            runner.run_host(pinned, cameras=cams)
+        h2d = 48 * nj  # rows 0..2 of each job's model-view
     else:
         host = pinned.numpy()
 
         def e2e_step():
             for i, (mid, mv, W, H) in enumerate(jobs):
                 r.render_into_host(mid, W, H, host[3 * offs[i]:3 * offs[i + 1]], mv=mv, mode=mode)
+        h2d = None  # each call uploads its one-job table (camera included)
     for _ in range(max(1, args.warmup)):
         e2e_step()
     t0 = time.perf_counter()
@@ -384,16 +658,9 @@ def run_ours(args, rank, world, dist):
         "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": round(float(t_main / K), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded meshes, TF and views)",
-        "config": {"workload": wl["name"], "desc": wl["desc"], "form": args.form,
-                   "meshes": [{"cells": p["n"], "tets": int(p["tet"].shape[0]),
-                               "verts": int(p["vert"].shape[0]),
-                               "ext_faces": int(p["extf"].shape[0])} for p in wl["meshes"]],
-                   "jobs": nj, "pixels_per_step": int(npix), "rays_per_step": rays_step,
-                   "tet_steps_per_step": steps_step,
-                   "mode": ("composited (every entry segment, depth-ordered)" if args.mode == "composited"
-                            else "reference (last visible face wins)"),
-                   "l2": "flushed between timed steps (256 MiB write, untimed)",
-                   "parallelism": f"{world} replica(s), one per GPU", "tuning": tuning},
+        "config": workload_config(wl, rays_step, args.mode),
+        "run": {"form": args.form, "parallelism": f"{world} replica(s), one per GPU",
+                "tuning": tuning, "tet_steps_per_step": steps_step},
         "fps": round(float(nj * world * K / (t_main * 1e-3)), 2),
         "gsteps_per_s": round(float(steps_step * world * K / (t_main * 1e-3) / 1e9), 3),
         "batched": {"value": round(float(mrays(t_batch, kp)), 2), "unit": "Mrays/s",
@@ -401,8 +668,12 @@ def run_ours(args, rank, world, dist):
         "plain_per_view": {"value": round(float(mrays(t_plain, kp)), 2), "unit": "Mrays/s",
                            "ms_per_step": round(float(t_plain / kp), 3)},
         "batched_over_plain": round(float(t_plain / t_batch), 3),
-        "e2e": {"value": round(float(e2e), 2), "unit": "Mrays/s", "h2d_bytes_per_step": 64 * nj,
-                "d2h_bytes_per_step": int(npix * 3), "ms_per_step": round(float(t_e2e / K), 3)},
+        "e2e": {"value": round(float(e2e), 2), "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(npix * 3), "ms_per_step": round(float(t_e2e / K), 3),
+                "copies": ("per step: one 2D copy of the jobs' cameras (host to device), the "
+                           "batch graph, one copy of all RGB8 images (device to host)"
+                           if args.form == "batched" else
+                           "per job: its job table in, its RGB8 image out")},
         "gpu_launches": int(launches_per_step * K),
         "roofline": roof,
         "clocks": clk.summary(),
@@ -418,7 +689,7 @@ def run_served(args):
     from vfray_b200 import serve, synth
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
-    wl = make_workload("served")
+    wl = prepare_ours(workload_spec("mixed"))
     r, stream, mids = setup_gpu(wl, dev)
     rng = np.random.default_rng(7)
     res = (256, 512, 1024)
@@ -471,93 +742,6 @@ def run_served(args):
             "clocks": clk.summary()}
 
 
-# ------------------------------------------------------------------ reference (CPU)
-
-def reference_sample(wl, seconds, threads=0):
-    """The reference's CPU kernels (oracle/_ref, its own -O3 -ffast-math flags)
-    on all host cores over the workload's jobs in order, until ``seconds``
-    have passed (at least one job).  Per job: rotateVolume, normalizeVertices
-    and buildLmt of the reference, then its three stages."""
-    import oracle
-
-    R = oracle.Reference("fast")
-    nthreads = threads or os.cpu_count() or 1
-    done = 0
-    t0 = time.perf_counter()
-    R.set_tf(wl["tf"])
-    for (m, mv, W, H) in wl["jobs"]:
-        p = wl["meshes"][m]
-        R.set_mesh(p["vert"], p["tet"])
-        if mv is not None:
-            R.rotate(mv)
-            R.normalize()
-        R.set_con(p["con"], p["extf"].shape[0])
-        R.set_extf(p["extf"])
-        R.build_lmt()
-        R.render_mt(W, H, threads=nthreads)
-        done += 1
-        if time.perf_counter() - t0 >= seconds:
-            break
-    return done, time.perf_counter() - t0, nthreads
-
-
-def count_rays(wl, njobs):
-    """Rays (pixels with an entry face) per job, from the oracle's winner pass."""
-    import oracle
-    import vfray_b200 as vb
-
-    Or = oracle.Oracle()
-    out = []
-    for (m, mv, W, H) in wl["jobs"][:njobs]:
-        p = wl["meshes"][m]
-        v = p["vert"] if mv is None else vb.normalize(vb.rotate(p["vert"], mv))
-        om = Or.mesh(v, p["tet"], p["con"], p["extf"], wl["tf"], wl["psi"], p["lmt"][0])
-        out.append(int((Or.winners(om, W, H) >= 0).sum()))
-    return out
-
-
-def cpu_baseline(wl, seconds):
-    done, dt, nthreads = reference_sample(wl, seconds)
-    rays = sum(count_rays(wl, done))
-    return {"value": round(rays / dt / 1e6, 4), "unit": "Mrays/s", "cores": nthreads,
-            "kind": "reference",
-            "sample": f"{done} of {len(wl['jobs'])} jobs, reference vfRayKernelCPU.cc "
-                      f"(-O3 -ffast-math) on {nthreads} threads (column strips), {dt:.1f} s"}
-
-
-def run_reference(args, rank):
-    if rank != 0:
-        return None
-    import oracle
-
-    if not oracle.ref_available("fast"):
-        return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}
-    wl = make_workload("mixed" if args.workload == "served" else args.workload, args.views)
-    per_step_s = max(1.0, args.cpu_seconds / 4)
-    for _ in range(args.warmup):
-        reference_sample(wl, 0.0)
-    total_rays, total_t, nthreads, jobs_done = 0, 0.0, 1, 0
-    for _ in range(args.steps):
-        done, dt, nthreads = reference_sample(wl, per_step_s)
-        total_rays += sum(count_rays(wl, done))
-        total_t += dt
-        jobs_done += done
-    v = total_rays / total_t / 1e6
-    return {"impl": "reference", "metric": f"Mrays/s ({wl['desc']})", "value": round(v, 4),
-            "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(total_t / args.steps * 1e3, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded meshes, TF and views)",
-            "config": {"workload": wl["name"], "desc": wl["desc"],
-                       "jobs_per_step": "bounded sample (the first jobs of the workload)"},
-            "cpu_baseline": {"value": round(v, 4), "unit": "Mrays/s", "cores": nthreads,
-                             "kind": "reference",
-                             "sample": f"{jobs_done} jobs over {args.steps} steps, reference "
-                                       f"vfRayKernelCPU.cc (-O3 -ffast-math) on {nthreads} threads"},
-            "e2e": {"value": round(v, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
-
-
 def _json(o):
     return json.dumps(o, default=lambda x: x.item() if hasattr(x, "item") else str(x))
 
@@ -598,7 +782,7 @@ def main():
             dist.destroy_process_group()
         return
     out, wl = res
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         out["cpu_baseline"] = cpu_baseline(wl, args.cpu_seconds)
         if args.mode == "composited":
             out["cpu_baseline"]["sample"] += (" (its own last-visible-face render: the reference "

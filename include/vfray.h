@@ -41,20 +41,25 @@ extern "C" {
 #define VFR_ERR_BUDGET (-8)   /* request exceeds the memory budget */
 #define VFR_ERR_TIMEOUT (-9)  /* a bounded device wait gave up */
 
-/* Device status word bits (vfr_render_stats.device_status). */
-#define VFR_DEV_ABANDON 1u    /* adjacency did not point back (reference :365 return) */
-#define VFR_DEV_STEP_CAP 2u   /* a ray hit the per-ray step cap */
+/* Device status word bits (vfr_render_stats.device_status).  Bit 1 is not
+ * used: a mesh whose adjacency does not point back, on which the reference
+ * abandons the rest of a face (vfRayKernelCPU.cc:359-365), is refused at
+ * upload instead (VFR_ERR_MESH). */
+#define VFR_DEV_STEP_CAP 2u   /* a ray hit the per-ray step cap (VFR_OPT_STEP_CAP) */
 #define VFR_DEV_RANGE 4u      /* an id read on the device was out of range */
-#define VFR_DEV_QUEUE 8u      /* a bounded work-queue wait gave up */
+#define VFR_DEV_QUEUE 8u      /* a bounded wait of the served kernel for work gave up */
 #define VFR_DEV_OVERFLOW 16u  /* an entry list exceeded its capacity */
+#define VFR_DEV_CYCLE 32u     /* a ray's walk came back to a (tet, entry face) state it had
+                                 left: the reference's loop would never end; the pixel keeps
+                                 what the ray composited before it was stopped */
 
-/* Options (vfr_set_option). */
+/* Options (vfr_set_option).  Number 2 is not used. */
 #define VFR_OPT_STEP_CAP 1        /* per-ray tet-walk cap; 0 = 4*nT + 64 (default) */
-#define VFR_OPT_QUEUE_CHUNK 2     /* rays a warp takes from the work queue at a time (32) */
 #define VFR_OPT_BLOCKS_PER_SM 3   /* traversal CTAs per SM; 0 = occupancy maximum */
 #define VFR_OPT_PROFILE 4         /* 1: record per-stage CUDA events of every view */
 #define VFR_OPT_TRAVERSE_VARIANT 5 /* traversal register budget: 0 = 2 CTAs/SM, 1 = 3 CTAs/SM (1) */
-#define VFR_OPT_REFILL 6          /* refill a warp's idle lanes once >= this many are idle (4) */
+#define VFR_OPT_REFILL 6          /* queue chunk: a warp takes rays from the work queue once at
+                                     least this many of its lanes are idle, one per idle lane (4) */
 #define VFR_OPT_RASTER_WARPS 7    /* stage (b) warps per SM (64) */
 #define VFR_OPT_TILE_WIDTH 8      /* ray-list screen tile width: 4, 8, 16, 32 (4 = 4x8) */
 
@@ -98,8 +103,10 @@ VFR_API int vfr_profile_read(vfr_ctx* ctx, float* ms3, int cap, int* count);
 /* ---- tables (vfRay.cu:266-285 uploads the TF and the psi cudaArray) ---- */
 
 /* tf256x4: 256 RGBA entries (vfRayPreComp.cc:551-579 reads them).
- * psi512x512: the psi(gamma) table, [front][back]; NULL selects the table
- * this library generates (see vfr_psi_table). */
+ * psi512x512: the psi(gamma) table, [front][back]; NULL selects the
+ * reference's own table (vfr_psi_table_reference), and fails with
+ * VFR_ERR_IO where the library was built without it -- pass the table this
+ * library generates (vfr_psi_table) there. */
 VFR_API int vfr_tables_upload(vfr_ctx* ctx, const float* tf256x4, const float* psi512x512);
 
 /* ---- meshes ------------------------------------------------------------ */
@@ -107,10 +114,12 @@ VFR_API int vfr_tables_upload(vfr_ctx* ctx, const float* tf256x4, const float* p
 /* Replaces prepareDevice1 + the initCUDA uploads (vfRay.cu:256-307).  The
  * arrays are copied; the mesh stays resident until released.  Validates ids,
  * adjacency symmetry and the external-face list (VFR_ERR_MESH on failure:
- * the reference would walk such a mesh into its :365 `return`).  maxZ/minZ
- * are accepted for the .lmt layout; only maxEdge enters the render, and it
- * must be below 2^80 (VFR_ERR_INVALID otherwise; a normalised mesh has at
- * most 2 sqrt 3).  At most 2^27 vertices. */
+ * the reference would walk such a mesh into its :365 `return`, which
+ * abandons the rest of a face; this library refuses the mesh instead).
+ * maxZ/minZ are accepted for the .lmt layout; only maxEdge enters the
+ * render, and it must be below 2^80 (VFR_ERR_INVALID otherwise; a
+ * normalised mesh has at most 2 sqrt 3).  At most 2^27 vertices and fewer
+ * than 2^30 tets. */
 VFR_API int vfr_mesh_upload(vfr_ctx* ctx, const float* vert4, uint32_t nV, const uint32_t* tet4,
                     const uint32_t* con4, uint32_t nT, const uint32_t* extf2, uint32_t nExt,
                     float maxEdge, float maxZ, float minZ, int* mesh_id);
@@ -191,8 +200,18 @@ VFR_API int vfr_batch_stats(vfr_batch* b, vfr_render_stats* per_job, uint32_t n)
 /* Device output pointers of a job (the batch's own when it owns them). */
 VFR_API int vfr_batch_output(vfr_batch* b, uint32_t job, uint8_t** rgb8_dev, float** rgba_dev,
                              uint32_t** steps_dev);
+/* Replaces the model-view of every job (n = the batch's job count): one
+ * asynchronous host-to-device copy on the context stream of the first three
+ * rows of each matrix, after which the next vfr_batch_run -- a replayed
+ * graph included -- renders with the new cameras.  mv16: n row-major 4x4
+ * matrices in host memory (pinned memory gives a full-speed copy), left
+ * unchanged until the copy has run (vfr_batch_read or vfr_synchronize).
+ * Only jobs given a model-view at vfr_batch_set_jobs (use_mv) use theirs. */
+VFR_API int vfr_batch_set_cameras(vfr_batch* b, const float* mv16, uint32_t n);
 /* Copies every job's outputs to host buffers, concatenated in job order
- * (any may be NULL), and waits: the host-buffer end of a batch. */
+ * (any may be NULL), and waits: the host-buffer end of a batch.  Outputs
+ * that lie back to back on the device (those the batch owns) come back in
+ * one copy per kind. */
 VFR_API int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host,
                            uint32_t* steps_host);
 /* Autotuner: times stages (b) and (c) of the batch over a grid of the
@@ -266,10 +285,13 @@ VFR_API void vfr_server_destroy(vfr_server* s);
  * the default stream).  Its scratch is a fixed device array inside the
  * library (32 bytes per external face for up to VFR_STATIC_MAX_EXT faces,
  * about 8 MiB, held on every GPU that loads the library until exit); larger
- * meshes get VFR_ERR_BUDGET.  The first call on a device looks that array's
- * address up, so make it before any stream capture.  Calls share the array:
- * calls that overlap on the GPU race.  An external face whose ids are out of
- * range counts as not visible.  Calls no cudaMalloc/cudaFree. */
+ * meshes get VFR_ERR_BUDGET.  The array's device address belongs to the
+ * current CUDA context: a call whose stream is not capturing looks it up in
+ * that context, and a call under stream capture uses the address an earlier
+ * call found in the same context (VFR_ERR_STATE if none did).  Calls share
+ * the array: calls that overlap on the GPU race.  An external face whose ids
+ * are out of range counts as not visible.  Output pointers must be 4-byte
+ * aligned (VFR_ERR_INVALID).  Calls no cudaMalloc/cudaFree. */
 #define VFR_STATIC_MAX_EXT (1u << 18)
 VFR_API int vfr_find_visible_static(const float* vert4_dev, uint32_t nV, const uint32_t* tet4_dev,
                                     uint32_t nT, const uint32_t* extf2_dev, uint32_t nExt,
@@ -281,6 +303,12 @@ VFR_API int vfr_find_visible_static(const float* vert4_dev, uint32_t nV, const u
  * int_0^1 exp(-(tf*u + (tb - tf)*u^2/2)) du at gamma = i/512, tau =
  * gamma/(1-gamma), truncated to 7 decimals like psiGammaTable512.h. */
 VFR_API int vfr_psi_table(float* out512x512);
+/* The reference's own psi table (psiGammaTable512.h:10-20, which
+ * vfRay.cu:280-284 uploads), as converted at build time from the reference
+ * sources into data/psiGammaTable512.bin beside this library (with the
+ * table's copyright notice in data/psiGammaTable512.NOTICE), or read from
+ * the file $VFRAY_PSI_TABLE names.  VFR_ERR_IO if there is no such file. */
+VFR_API int vfr_psi_table_reference(float* out512x512);
 /* normalizeVertices (vfRayPreComp.cc:84-145), in place. */
 VFR_API int vfr_normalize(float* vert4, uint32_t nV);
 /* rotateVolume (vfRayPreComp.cc:886-906), in place; mv16 row-major. */

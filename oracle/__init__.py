@@ -21,7 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_bin", "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
-REF_SOURCES = "/root/reference"
+# the reference sources (only present where the oracle is built from them)
+REF_SOURCES = os.environ.get("VFRAY_REF", "/root/reference")
 
 _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
@@ -36,7 +37,7 @@ def build(reference: bool = True) -> None:
     targets = ["oracle"]
     if reference and os.path.isdir(REF_SOURCES):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"VFRAY_REF={REF_SOURCES}", *targets], check=True)
 
 
 def ref_available(variant: str = "strict") -> bool:
@@ -54,7 +55,7 @@ class _VoMesh(C.Structure):
     _fields_ = [("vert", C.c_void_p), ("tet", C.c_void_p), ("con", C.c_void_p),
                 ("extf", C.c_void_p), ("nV", C.c_uint32), ("nT", C.c_uint32),
                 ("nExt", C.c_uint32), ("tf", C.c_void_p), ("psi", C.c_void_p),
-                ("maxEdge", C.c_float)]
+                ("maxEdge", C.c_float), ("step_cap", C.c_uint32)]
 
 
 class Oracle:
@@ -71,14 +72,14 @@ class Oracle:
         L.vo_compact.restype = C.c_uint32
 
     @staticmethod
-    def mesh(vert, tet, con, extf, tf, psi, max_edge):
+    def mesh(vert, tet, con, extf, tf, psi, max_edge, step_cap=0):
         arrs = [np.ascontiguousarray(vert, np.float32), np.ascontiguousarray(tet, np.uint32),
                 np.ascontiguousarray(con, np.uint32), np.ascontiguousarray(extf, np.uint32),
                 np.ascontiguousarray(tf, np.float32), np.ascontiguousarray(psi, np.float32)]
         m = _VoMesh(arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data,
                     arrs[3].ctypes.data, arrs[0].size // 4, arrs[1].size // 4,
                     arrs[3].size // 2, arrs[4].ctypes.data, arrs[5].ctypes.data,
-                    float(max_edge))
+                    float(max_edge), int(step_cap))
         m._keep = arrs
         return m
 
@@ -180,6 +181,12 @@ class Reference:
         t = np.ascontiguousarray(tet, np.uint32)
         self.lib.ref_set_mesh(v.ctypes.data_as(C.c_void_p), C.c_uint32(v.size // 4),
                               t.ctypes.data_as(C.c_void_p), C.c_uint32(t.size // 4))
+
+    def set_vert(self, vert):
+        """Replace the vertices (same count as the current mesh)."""
+        v = np.ascontiguousarray(vert, np.float32)
+        assert v.size == 4 * self.lib.ref_num_verts()
+        self.lib.ref_set_vert(v.ctypes.data_as(C.c_void_p))
 
     def vert(self):
         out = np.zeros((self.lib.ref_num_verts(), 4), np.float32)

@@ -78,6 +78,9 @@ API int ref_set_mesh(const float* v, uint nv, const uint* t, uint nt) {
   return 0;
 }
 API void ref_get_vert(float* v) { std::memcpy(v, h_vertList, sizeof(real) * 4 * (size_t)numVerts); }
+// Restores the vertices only (same count), e.g. the normalised mesh before
+// the next view's rotateVolume.
+API void ref_set_vert(const float* v) { std::memcpy(h_vertList, v, sizeof(real) * 4 * (size_t)numVerts); }
 API uint ref_num_verts(void) { return numVerts; }
 API uint ref_num_tets(void) { return numTets; }
 API uint ref_num_ext(void) { return numExtFaces; }

@@ -65,6 +65,7 @@ static void plane(f4 a, f4 b, f4 c, vo_face* f) {
 
 static int mesh_ok(const vo_mesh* m) {
   if (!m || !m->vert || !m->tet || !m->con || !m->extf || !m->tf || !m->psi) return 0;
+  if (m->nT >= (1u << 30)) return 0; /* walk states are packed as tet << 2 | face */
   for (size_t i = 0; i < 4 * (size_t)m->nT; ++i)
     if (m->tet[i] >= m->nV || m->con[i] >= m->nT) return 0;
   for (uint32_t e = 0; e < m->nExt; ++e)
@@ -233,17 +234,42 @@ static void ray64_step(const vo_mesh* m, f4 a, f4 b, f4 c, ray64* D) {
   D->zp = zn;
 }
 
+/* Iterations a ray runs before its walk is watched for a repeated state,
+ * and its cap (4 nT + 64, or the mesh's step_cap).  The walk from a state
+ * (tet, entry face) is fixed for a pixel, so a state that comes back means
+ * the reference's loop never ends.  Past the threshold the state is saved at
+ * every power-of-two iteration count and compared with every later one
+ * (Brent).  The CUDA traversal applies the same rule. */
+#define WATCH_STEPS 4095u
+
+static uint32_t step_cap(const vo_mesh* m) {
+  if (m->step_cap) return m->step_cap;
+  uint64_t c = 4ull * m->nT + 64u;
+  return c > 0x7fffffffu ? 0x7fffffffu : (uint32_t)c;
+}
+
 /* One ray segment from entry (t, f) with entry depth/scalar (zp, sp),
- * :276-542.  Returns 0, or -1 on the :365 `return` (adjacency that does
- * not point back). */
+ * :276-542.  Returns 0; -1 on the :365 `return` (adjacency that does not
+ * point back); TRACE_CAP or TRACE_CYCLE when the ray was stopped (the
+ * reference would go on forever). */
+#define TRACE_CAP 1
+#define TRACE_CYCLE 2
 static int trace(const vo_mesh* m, float ox, float oy, uint32_t t, uint32_t f, float zpx,
                  float zpy, ray_state* R, ray64* D) {
   f4 cb = tfget(m, zpy);
   if (D) ray64_begin(m, t, f, D);
   uint32_t tpx = t, tpy = f;
+  const uint32_t cap = step_cap(m), watch = cap < WATCH_STEPS ? cap : WATCH_STEPS;
+  uint32_t saved = 0xffffffffu;
   R->lastZ = zpx;
   for (;;) {
     R->iters++;
+    if (R->iters > watch) {
+      if (R->iters > cap) return TRACE_CAP;
+      const uint32_t key = (tpx << 2) | tpy;
+      if (key == saved) return TRACE_CYCLE;
+      if ((R->iters & (R->iters - 1u)) == 0u) saved = key;
+    }
     uint32_t tny = tpy, tnx;
     f4 fv[4];
     for (int k = 0; k < 4; ++k) fv[k] = vget(m, m->tet[4 * (size_t)tpx + k]);
@@ -544,10 +570,11 @@ static void comp_range(void* c_, size_t lo, size_t hi) {
     for (size_t i = 0; i < n; ++i) {
       if (L[i].z > exitZ) continue;
       uint32_t e = L[i].e;
-      if (trace(c->m, ox, oy, c->m->extf[2 * e], c->m->extf[2 * e + 1], L[i].z, L[i].s, &R, NULL) < 0)
-        __atomic_store_n(&c->err, 1, __ATOMIC_RELAXED);
+      int rc = trace(c->m, ox, oy, c->m->extf[2 * e], c->m->extf[2 * e + 1], L[i].z, L[i].s, &R, NULL);
+      if (rc < 0) __atomic_store_n(&c->err, 1, __ATOMIC_RELAXED);
       exitZ = R.lastZ;
       ++segs;
+      if (rc > 0) break; /* stopped: the ray ends with what it composited */
     }
     finalize(&R, c->rgb8 ? c->rgb8 + 3 * p : NULL, c->rgba ? c->rgba + 4 * p : NULL);
     if (c->steps) c->steps[p] = R.iters;

@@ -29,6 +29,7 @@ typedef struct {
   const float* tf;       /* 256 x RGBA */
   const float* psi;      /* 512 x 512, [front][back] */
   float maxEdge;
+  uint32_t step_cap;     /* per-ray iteration cap; 0 = 4 nT + 64 */
 } vo_mesh;
 
 /* Stage (a), vfRayKernelCPU.cc:51-132: plane coefficients and back-face
@@ -41,7 +42,12 @@ uint32_t vo_compact(const vo_face* faces, uint32_t nExt, uint32_t* visExt);
 void vo_project(const vo_mesh* m, const uint32_t* visExt, uint32_t nVis,
                 uint32_t W, uint32_t H, uint32_t* bbox4);
 
-/* Stage (c) in reference order (main.cc:209-218, vfRayKernelCPU.cc:173-566):
+/* Every traversal below stops a ray whose walk comes back to a (tet, entry
+ * face) state, checked from iteration 4096 on, or that reaches the step cap;
+ * the reference's loop never ends on such a ray.  The ray keeps what it
+ * composited before the stop, and its steps count the stopping iteration.
+ *
+ * Stage (c) in reference order (main.cc:209-218, vfRayKernelCPU.cc:173-566):
  * faces in visible order, each over its box, x outer / y inner, with the
  * column break on an out-of-range entry scalar (:274), the face abandon on
  * inconsistent adjacency (:365) and last-writer-wins per pixel.

@@ -10,7 +10,6 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 GOLDEN_CASES = ["convex6_rot", "carved10_rot", "convex5_axis", "single_tet", "cfg0_convex24"]
-REF_SOURCES = "/root/reference"
 
 
 def pytest_configure(config):
@@ -19,7 +18,9 @@ def pytest_configure(config):
 
 
 def has_reference_sources():
-    return os.path.isdir(REF_SOURCES)
+    import oracle
+
+    return os.path.isdir(oracle.REF_SOURCES)
 
 
 def load_golden(name):

@@ -14,6 +14,11 @@ the inputs (small cases) or an input checksum (the 24^3 case, regenerated from
 its seeds), and the reference outputs: RGB8 image, per-pixel last writer
 (ext-face index), visible ext faces in order, bounding boxes, and per-face
 compositing-step counts (from the counting build).
+
+    python tests/golden/make_golden.py reftable
+
+writes reftable.npz: the same cases rendered by the reference with its own
+psi table (psiGammaTable512.h), the library's default table.
 """
 import hashlib
 import os
@@ -63,6 +68,46 @@ def make_inputs(name):
     return vert, tet, synth.transfer_function(2)
 
 
+def main_reftable():
+    """reftable.npz: every case rendered by the reference with its own psi
+    table (psiGammaTable512.h as compiled into the reference build), strict
+    and fast-math builds, and the table's checksum; the geometry (visible
+    set, writers, steps) does not depend on the table and stays in the
+    per-case fixtures."""
+    refs = {v: oracle.Reference(v) for v in ("strict", "fast")}
+    own = refs["strict"].psi()
+    assert np.array_equal(own, refs["fast"].psi())
+    rec = dict(psi_sha256=checksum(own))
+    for name, (n, carved, vs, W, H, store) in CASES.items():
+        d = dict(np.load(os.path.join(OUT, f"{name}.npz")))
+        if "vert" in d:
+            vn, tet, con, extf, tf = d["vert"], d["tet"], d["con"], d["extf"], d["tf"]
+        else:
+            vert, tet, tf = make_inputs(name)
+            R = refs["strict"]
+            R.set_mesh(vert, tet)
+            R.normalize()
+            R.build_con()
+            R.build_extf()
+            con, _ = R.con()
+            extf, vn = R.extf(), R.vert()
+        assert checksum(vn, tet, con, extf, tf) == str(d["input_sha256"])
+        for k, r in refs.items():
+            r.set_psi(own)
+            r.set_mesh(vn, tet)
+            r.set_con(con, int(d["n_ext"]))
+            r.set_extf(extf)
+            r.set_lmt(*d["lmt"])
+            r.set_tf(tf)
+            o = r.render(int(W), int(H), detect=(k == "strict"))
+            rec[f"{name}_{k}"] = o["rgb8"]
+            if k == "strict":
+                assert np.array_equal(o["writer"], d["writer"]), name
+    path = os.path.join(OUT, "reftable.npz")
+    np.savez_compressed(path, **rec)
+    print(f"reftable: {len(CASES)} cases -> {os.path.getsize(path)} bytes")
+
+
 def main():
     psi = psi_table()
     refs = {v: oracle.Reference(v) for v in ("strict", "count", "fast")}
@@ -100,4 +145,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["reftable"]:
+        main_reftable()
+    else:
+        main()

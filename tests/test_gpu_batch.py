@@ -127,3 +127,75 @@ def test_batch_with_rayless_jobs(renderer):
                     B.close()
     finally:
         renderer.release_mesh(mid)
+
+
+def test_cameras_change_between_host_runs(renderer, scene):
+    """The host-buffer form uploads the step's cameras: a replayed graph
+    renders with the model-views of the latest vfr_batch_set_cameras, and
+    each job equals the same view rendered alone with that camera."""
+    import torch
+
+    jobs = [j for j in scene if j[1] is not None]
+    npx = sum(W * H for (_, _, W, H) in jobs)
+    B = vbatch.BatchRenderer(renderer, jobs)
+    try:
+        B.prepare()
+        rgb = torch.empty(npx * 3, dtype=torch.uint8, pin_memory=True)
+        cams = torch.empty((len(jobs), 4, 4), dtype=torch.float32, pin_memory=True)
+        images = []
+        for views in (synth.orbit_views(len(jobs), seed=21), synth.orbit_views(len(jobs), seed=22)):
+            cams.copy_(torch.from_numpy(views))
+            B.run_host(rgb, cameras=cams)
+            B.stats()
+            img = rgb.numpy().copy()
+            images.append(img)
+            off = 0
+            for j, (mid, _, W, H) in enumerate(jobs):
+                single = renderer.render(mid, W, H, mv=views[j])
+                n = W * H
+                assert np.array_equal(img[3 * off:3 * (off + n)].reshape(H, W, 3), single["rgb8"]), j
+                off += n
+        assert not np.array_equal(images[0], images[1])
+    finally:
+        B.close()
+
+
+def test_cycling_ray_is_stopped(renderer, oracle_lib):
+    """A mesh whose tets list their vertices in random order, seen from a
+    view where one ray's walk cycles among the tets around an edge (the
+    reference's loop never ends on it): the ray is stopped by the exact
+    cycle check (its state saved at power-of-two iteration counts from 4096
+    on), its pixel keeps what it composited, the status says so, and every
+    pixel's step count -- the cycling ray's included -- equals the oracle's,
+    which applies the same rule."""
+    vert, tet = synth.make_mesh(12, carved=False, view_seed=None)
+    tet = synth.permute_tet_vertices(tet, 0)
+    p = vb.prepare(vert, tet)
+    tf = synth.transfer_function(2)
+    psi = vb.psi_table()
+    mv = synth.orbit_views(8, seed=3)[5]
+    renderer.upload_tables(tf, psi)
+    mid = renderer.upload_mesh(p["vert"], p["tet"], p["con"], p["extf"], p["lmt"])
+    try:
+        v = vb.normalize(vb.rotate(p["vert"], mv))
+        m = oracle_lib.mesh(v, p["tet"], p["con"], p["extf"], tf, psi, vb.build_lmt(v, p["tet"])[0])
+        o = oracle_lib.render_ref(m, 256, 256)
+        assert int((o["steps"] > 4095).sum()) == 1  # the one cycling ray
+        B = vbatch.BatchRenderer(renderer, [(mid, mv, 256, 256)])
+        try:
+            B.prepare()
+            B.run()
+            with pytest.raises(vb.VfrError, match="cycle=32"):
+                B.stats()
+            steps = np.empty(256 * 256, np.uint32)
+            rgb = np.empty(256 * 256 * 3, np.uint8)
+            B.read(rgb8=rgb, steps=steps)
+            assert np.array_equal(steps.reshape(256, 256), o["steps"])
+            d = np.abs(rgb.reshape(256, 256, 3).astype(int) - o["rgb8"].astype(int)).max()
+            assert d <= 2, d
+        finally:
+            B.close()
+        # the context is usable afterwards
+        renderer.render(mid, 64, 64)
+    finally:
+        renderer.release_mesh(mid)

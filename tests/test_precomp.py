@@ -109,11 +109,74 @@ def test_psi_table_against_reference_table():
     assert ours[0, 0] == 1.0 and ours.dtype == np.float32
     if not has_reference_sources():
         pytest.skip("reference sources absent")
-    ref = vb.read_psi_source("/root/reference/psiGammaTable512.h")
+    import oracle
+
+    ref = vb.read_psi_source(os.path.join(oracle.REF_SOURCES, "psiGammaTable512.h"))
     bad = np.argwhere(ours != ref)
     band = bad[:, 1] - bad[:, 0]
     assert len(bad) < 600 and band.min() >= 0 and band.max() <= 9
     assert np.abs(ours - ref).max() < 3.3e-3
+
+
+def test_reference_psi_table_is_shipped():
+    """The library's default psi table is the reference's own: the build
+    converts psiGammaTable512.h into vfray_b200/data/ (with its notice), and
+    its checksum is the one the reference-table fixtures were rendered with."""
+    import oracle
+    from tests.golden.make_golden import checksum
+
+    data = os.path.join(os.path.dirname(vb.__file__), "data")
+    if not os.path.exists(os.path.join(data, "psiGammaTable512.bin")):
+        assert not has_reference_sources(), "the build did not convert the reference's psi table"
+        pytest.skip("library built without the reference sources")
+    t = vb.reference_psi_table()
+    fx = np.load(os.path.join(os.path.dirname(__file__), "golden", "reftable.npz"))
+    assert checksum(t) == str(fx["psi_sha256"])
+    assert "Sandia" in open(os.path.join(data, "psiGammaTable512.NOTICE")).read()
+    if has_reference_sources():
+        src = vb.read_psi_source(os.path.join(oracle.REF_SOURCES, "psiGammaTable512.h"))
+        assert np.array_equal(t, src)
+        assert np.array_equal(t, oracle.Reference("strict").psi())
+
+
+@pytest.mark.parametrize("n,carved,perm", [(4, False, None), (6, True, 5), (8, False, 2),
+                                            (12, True, None), (24, True, 1)])
+def test_numpy_adjacency_restatement(n, carved, perm, tmp_path):
+    """oracle.precomp (the numpy restatement the benchmark's reference arm
+    prepares its inputs with, without loading the product library) gives
+    the library's adjacency and external faces -- and the reference's own,
+    where its sources are present -- and its text files read back through
+    the reference's readers as the same arrays."""
+    import oracle
+    from oracle import precomp
+
+    vert, tet = synth.make_mesh(n, carved=carved, view_seed=None)
+    if perm is not None:
+        tet = synth.permute_tet_vertices(tet, perm)
+    con, n_ext = precomp.build_con(tet)
+    extf = precomp.build_extf(con)
+    lc, ln = vb.build_con(tet, vert.shape[0])
+    assert np.array_equal(con, lc) and n_ext == ln
+    assert np.array_equal(extf, vb.build_extf(lc))
+    if not has_reference_sources() or n > 12:
+        return
+    R = _ref()
+    R.set_mesh(vert, tet)
+    R.build_con()
+    R.build_extf()
+    rcon, rn = R.con()
+    assert np.array_equal(con, rcon) and n_ext == rn and np.array_equal(extf, R.extf())
+    tf = synth.transfer_function(2)
+    precomp.write_off(str(tmp_path / "m.off"), vert, tet)
+    precomp.write_con(str(tmp_path / "m.con"), con, n_ext)
+    precomp.write_extf(str(tmp_path / "m.extf"), extf)
+    precomp.write_tf(str(tmp_path / "m.tf"), tf)
+    R2 = oracle.Reference("strict")
+    for kind in ("off", "con", "extf", "tf"):
+        getattr(R2, f"read_{kind}")(str(tmp_path / f"m.{kind}"))
+    assert np.array_equal(R2.vert(), vert)
+    assert np.array_equal(R2.con()[0], con) and R2.con()[1] == n_ext
+    assert np.array_equal(R2.extf(), extf) and np.array_equal(R2.tf(), tf)
 
 
 def test_build_con_rejects_degenerate_tets():

@@ -80,3 +80,7 @@ def test_static_rejects_oversize_and_bad_arguments():
     # misaligned vertex buffer
     bad = C.c_void_p(buf.data_ptr() + 4)
     assert lib.vfr_find_visible_static(bad, 4, p, 1, p, 4, p, p, None) == _lib.VFR_ERR_INVALID
+    # misaligned outputs (written with 4-byte stores): refused on the host
+    odd = C.c_void_p(buf.data_ptr() + 2)
+    assert lib.vfr_find_visible_static(p, 4, p, 1, p, 4, odd, p, None) == _lib.VFR_ERR_INVALID
+    assert lib.vfr_find_visible_static(p, 4, p, 1, p, 4, p, odd, None) == _lib.VFR_ERR_INVALID

@@ -16,14 +16,15 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (MODE_COMPOSITED, MODE_REF, OPT_BLOCKS_PER_SM, OPT_PROFILE,
-                   OPT_QUEUE_CHUNK, OPT_REFILL, OPT_STEP_CAP, OPT_TRAVERSE_VARIANT, RenderStats, VfrError, check, load, ptr,
-                   VFR_DEV_ABANDON, VFR_DEV_OVERFLOW, VFR_DEV_QUEUE, VFR_DEV_RANGE,
-                   VFR_DEV_STEP_CAP)
+from ._lib import (MODE_COMPOSITED, MODE_REF, OPT_BLOCKS_PER_SM, OPT_PROFILE, OPT_RASTER_WARPS,
+                   OPT_REFILL, OPT_STEP_CAP, OPT_TILE_WIDTH, OPT_TRAVERSE_VARIANT, RenderStats,
+                   VfrError, check, load, ptr, VFR_DEV_CYCLE, VFR_DEV_OVERFLOW, VFR_DEV_QUEUE,
+                   VFR_DEV_RANGE, VFR_DEV_STEP_CAP)
 
 __all__ = [
     "Renderer", "VfrError", "MODE_REF", "MODE_COMPOSITED", "RenderStats", "load",
-    "normalize", "rotate", "build_con", "build_extf", "build_lmt", "psi_table", "default_tf",
+    "normalize", "rotate", "build_con", "build_extf", "build_lmt", "psi_table",
+    "reference_psi_table", "default_tf",
     "prepare", "read_off", "read_con", "read_extf", "read_lmt", "read_tf", "write_off",
     "write_con", "write_extf", "write_lmt", "write_tf", "write_ppm", "read_psi_source",
     "write_mesh_cache", "read_mesh_cache", "clean_tf",
@@ -50,6 +51,16 @@ def psi_table() -> np.ndarray:
     """The generated 512x512 psi(gamma) table, [front][back]."""
     out = np.empty((512, 512), np.float32)
     check(load().vfr_psi_table(ptr(out)), what="vfr_psi_table")
+    return out
+
+
+def reference_psi_table() -> np.ndarray:
+    """The reference's own 512x512 psi table (psiGammaTable512.h), as the
+    build converted it from the reference sources into
+    vfray_b200/data/psiGammaTable512.bin (or the file $VFRAY_PSI_TABLE
+    names); raises VfrError if the library was built without it."""
+    out = np.empty((512, 512), np.float32)
+    check(load().vfr_psi_table_reference(ptr(out)), what="vfr_psi_table_reference")
     return out
 
 
@@ -275,6 +286,8 @@ class Renderer:
         return out[: n.value].copy()
 
     def upload_tables(self, tf, psi=None):
+        """The transfer function and the psi table; psi None: the
+        reference's own table (see reference_psi_table)."""
         tf = _f32(tf, (256, 4))
         psi = None if psi is None else _f32(psi, (512, 512))
         self._check(self.lib.vfr_tables_upload(self.h, ptr(tf), ptr(psi)), "vfr_tables_upload")

@@ -25,14 +25,13 @@ VFR_ERR_IO = -7
 VFR_ERR_BUDGET = -8
 VFR_ERR_TIMEOUT = -9
 
-VFR_DEV_ABANDON = 1
 VFR_DEV_STEP_CAP = 2
 VFR_DEV_RANGE = 4
 VFR_DEV_QUEUE = 8
 VFR_DEV_OVERFLOW = 16
+VFR_DEV_CYCLE = 32
 
 OPT_STEP_CAP = 1
-OPT_QUEUE_CHUNK = 2
 OPT_BLOCKS_PER_SM = 3
 OPT_PROFILE = 4
 OPT_TRAVERSE_VARIANT = 5
@@ -136,6 +135,7 @@ SIGNATURES = {
     "vfr_batch_stats": (_i, [_vp, C.POINTER(RenderStats), _u32]),
     "vfr_batch_output": (_i, [_vp, _u32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
     "vfr_batch_read": (_i, [_vp, _vp, _vp, _vp]),
+    "vfr_batch_set_cameras": (_i, [_vp, _vp, _u32]),
     "vfr_batch_autotune": (_i, [_vp, _i, C.POINTER(Tuning)]),
     "vfr_batch_scratch_bytes": (_i, [_vp, C.POINTER(C.c_uint64)]),
     "vfr_server_create": (_i, [_vp, C.c_uint64, _u32, C.POINTER(_vp)]),
@@ -145,6 +145,7 @@ SIGNATURES = {
     "vfr_server_destroy": (None, [_vp]),
     "vfr_find_visible_static": (_i, [_vp, _u32, _vp, _u32, _vp, _u32, _vp, _vp, _vp]),
     "vfr_psi_table": (_i, [_vp]),
+    "vfr_psi_table_reference": (_i, [_vp]),
     "vfr_normalize": (_i, [_vp, _u32]),
     "vfr_rotate": (_i, [_vp, _u32, _vp]),
     "vfr_build_con": (_i, [_vp, _u32, _u32, _vp, C.POINTER(_u32), _i]),

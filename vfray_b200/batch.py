@@ -110,9 +110,28 @@ class BatchRenderer:
         check(self.lib.vfr_batch_read(self.h, ptr(rgb8), ptr(rgba), ptr(steps)), self.r.h,
               "vfr_batch_read")
 
-    def run_host(self, rgb8_host):
-        """The host-buffer form: run, then read every job's RGB8 (pinned host
-        memory gives full copy bandwidth)."""
+    def set_cameras(self, mv):
+        """New model-views for every job, (njobs, 4, 4) row-major float32 in
+        host memory (a numpy array or a pinned torch tensor): copied to the
+        device asynchronously; the next run renders with them.  The buffer
+        must stay unchanged until the next read or synchronize."""
+        if hasattr(mv, "data_ptr"):
+            assert mv.dtype.is_floating_point and mv.element_size() == 4 and mv.is_contiguous()
+            assert mv.numel() == 16 * len(self.jobs)
+            p = C.c_void_p(mv.data_ptr())
+        else:
+            mv = np.ascontiguousarray(mv, np.float32).reshape(len(self.jobs), 16)
+            self._cams = mv  # alive until the copy has run
+            p = ptr(mv)
+        check(self.lib.vfr_batch_set_cameras(self.h, p, len(self.jobs)), self.r.h,
+              "vfr_batch_set_cameras")
+
+    def run_host(self, rgb8_host, cameras=None):
+        """The host-buffer form: cameras in (optional, see set_cameras), run,
+        then every job's RGB8 back into ``rgb8_host`` (pinned host memory
+        gives full copy bandwidth)."""
+        if cameras is not None:
+            self.set_cameras(cameras)
         self.run()
         self.read(rgb8=rgb8_host)
 

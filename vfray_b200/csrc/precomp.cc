@@ -6,6 +6,8 @@
 // O(nV * nT) (buildIncid + buildCon :219-501): sorted face triples bucketed by
 // their smallest vertex id give the same neighbour ids in O(nT log k).
 // Readers and writers keep the reference's text layouts byte for byte.
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
@@ -611,6 +613,31 @@ int vfr_read_psi_source(const char* path, float* out) {
     p = (size_t)(e - s);
   }
   return n == 512 * 512 ? VFR_OK : VFR_ERR_IO;
+}
+
+// The reference's own psi table as this library ships it: 512 x 512 raw
+// little-endian float32, [front][back], converted from psiGammaTable512.h by
+// bin/psiTable at build time and kept beside the library with the table's
+// copyright notice.  $VFRAY_PSI_TABLE names another such file.
+int vfr_psi_table_reference(float* out) {
+  if (!out) return VFR_ERR_INVALID;
+  std::string path;
+  if (const char* env = std::getenv("VFRAY_PSI_TABLE")) {
+    path = env;
+  } else {
+    Dl_info info;
+    if (!dladdr((void*)&vfr_psi_table_reference, &info) || !info.dli_fname) return VFR_ERR_IO;
+    path = info.dli_fname;
+    const size_t slash = path.rfind('/');
+    path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) +
+           "/data/psiGammaTable512.bin";
+  }
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return VFR_ERR_IO;
+  const size_t n = std::fread(out, sizeof(float), 512 * 512, f);
+  const bool more = std::fgetc(f) != EOF;
+  std::fclose(f);
+  return (n == 512 * 512 && !more) ? VFR_OK : VFR_ERR_IO;
 }
 
 // ---- writers ----

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -128,9 +129,9 @@ int Ctx::traverse_blocks_per_sm(int mode) {
 
 int Ctx::check_status(uint32_t status, uint32_t overflow) {
   if (overflow) return fail(VFR_ERR_DEVICE, "entry lists overflowed; render again");
-  if (status & (VFR_DEV_ABANDON | VFR_DEV_RANGE | VFR_DEV_STEP_CAP | VFR_DEV_OVERFLOW)) {
+  if (status & (VFR_DEV_CYCLE | VFR_DEV_RANGE | VFR_DEV_STEP_CAP | VFR_DEV_OVERFLOW)) {
     char buf[128];
-    std::snprintf(buf, sizeof buf, "device status 0x%x (abandon=1 step-cap=2 range=4 overflow=16)",
+    std::snprintf(buf, sizeof buf, "device status 0x%x (step-cap=2 range=4 overflow=16 cycle=32)",
                   status);
     return fail(VFR_ERR_DEVICE, buf);
   }
@@ -591,9 +592,6 @@ int vfr_set_option(vfr_ctx* c, int option, int64_t value) {
   if (value < 0 || value > 0x7fffffff) return C.fail(VFR_ERR_INVALID, "option value out of range");
   switch (option) {
     case VFR_OPT_STEP_CAP: C.step_cap = (uint32_t)value; return VFR_OK;
-    case VFR_OPT_QUEUE_CHUNK:
-      if (value < 1) return C.fail(VFR_ERR_INVALID, "queue chunk must be >= 1");
-      return VFR_OK;  // kept for the ABI: the refill kernel takes one ray per lane
     case VFR_OPT_BLOCKS_PER_SM: C.tune.blocks_per_sm = (uint32_t)value; return VFR_OK;
     case VFR_OPT_PROFILE: C.profile = value != 0; return VFR_OK;
     case VFR_OPT_TRAVERSE_VARIANT:
@@ -638,11 +636,14 @@ int vfr_profile_read(vfr_ctx* c, float* ms3, int cap, int* count) {
 int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
   CTX_OR_FAIL(c);
   if (!tf) return C.fail(VFR_ERR_INVALID, "transfer function is NULL");
-  std::vector<float> gen;
-  if (!psi) {
-    gen.resize(512 * 512);
-    vfr_psi_table(gen.data());
-    psi = gen.data();
+  std::vector<float> ref;
+  if (!psi) {  // the reference's own table, the drop-in default
+    ref.resize(512 * 512);
+    if (vfr_psi_table_reference(ref.data()) != VFR_OK)
+      return C.fail(VFR_ERR_IO,
+                    "the reference psi table (data/psiGammaTable512.bin beside the library, or "
+                    "$VFRAY_PSI_TABLE) is missing; pass vfr_psi_table's generated table instead");
+    psi = ref.data();
   }
   // the transfer function (256 float4) is followed by the 64 doubles
   // 2^(j/64) of the traversal's table-driven exponential
@@ -670,6 +671,8 @@ int vfr_mesh_upload(vfr_ctx* c, const float* vert4, uint32_t nV, const uint32_t*
   if (!vert4 || !tet4 || !con4 || (!extf2 && nExt) || !mesh_id || nV == 0 || nT == 0)
     return C.fail(VFR_ERR_INVALID, "mesh arrays missing or empty");
   if ((uint64_t)nExt > 4ull * nT) return C.fail(VFR_ERR_INVALID, "more external faces than faces");
+  // the traversal packs a walk state (tet, entry face) into 32 bits
+  if (nT >= (1u << 30)) return C.fail(VFR_ERR_INVALID, "2^30 tets or more");
   // the traversal divides depth steps (at least 1e-12) by it through a
   // reciprocal, exact while no quotient falls below 2^-126
   if (!(maxEdge < 0x1p80f)) return C.fail(VFR_ERR_INVALID, "maxEdgeLength not below 2^80");
@@ -1092,31 +1095,71 @@ int vfr_batch_autotune(vfr_batch* b, int reps, vfr_tuning* out) {
   return rc2;
 }
 
+int vfr_batch_set_cameras(vfr_batch* b, const float* mv16, uint32_t n) {
+  if (!b || !b->b.njobs) return VFR_ERR_STATE;
+  if (!b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  Batch& B = b->b;
+  if (!mv16 || n != B.njobs) return C.fail(VFR_ERR_INVALID, "one camera per job");
+  // the host copies follow, so a later layout of the same jobs keeps them
+  for (uint32_t j = 0; j < n; ++j) {
+    const float* m = mv16 + 16 * (size_t)j;
+    std::memcpy(B.specs[j].mv, m, sizeof B.specs[j].mv);
+    B.jobs[j].m0 = make_float4(m[0], m[1], m[2], m[3]);
+    B.jobs[j].m1 = make_float4(m[4], m[5], m[6], m[7]);
+    B.jobs[j].m2 = make_float4(m[8], m[9], m[10], m[11]);
+  }
+  // rows 0..2 of each matrix are the job table entry's first 48 bytes
+  static_assert(offsetof(vfr::JobDev, m0) == 0 && offsetof(vfr::JobDev, m2) == 32,
+                "job table camera layout");
+  return C.cuda(cudaMemcpy2DAsync(B.d_jobs.p, sizeof(vfr::JobDev), mv16, 16 * sizeof(float),
+                                  3 * sizeof(float4), n, cudaMemcpyHostToDevice, B.st()),
+                "camera upload");
+}
+
 int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host, uint32_t* steps_host) {
   if (!b || !b->b.njobs) return VFR_ERR_STATE;
   if (!b->owner) return VFR_ERR_STATE;
   Ctx& C = b->owner->impl;
   cudaSetDevice(C.device);
-  size_t off = 0;
-  int rc = VFR_OK;
-  for (uint32_t j = 0; j < b->b.njobs && !rc; ++j) {
-    const JobSpec& q = b->b.specs[j];
-    const size_t np = (size_t)q.W * q.H;
-    if (rgb8_host && q.rgb8)
-      rc = C.cuda(cudaMemcpyAsync(rgb8_host + 3 * off, q.rgb8, 3 * np, cudaMemcpyDeviceToHost,
-                                  C.stream),
-                  "rgb8 read");
-    if (!rc && rgba_host && q.rgba)
-      rc = C.cuda(cudaMemcpyAsync(rgba_host + 4 * off, q.rgba, sizeof(float4) * np,
-                                  cudaMemcpyDeviceToHost, C.stream),
-                  "rgba read");
-    if (!rc && steps_host && q.steps)
-      rc = C.cuda(cudaMemcpyAsync(steps_host + off, q.steps, sizeof(uint32_t) * np,
-                                  cudaMemcpyDeviceToHost, C.stream),
-                  "steps read");
-    off += np;
-  }
-  if (!rc) rc = C.cuda(cudaStreamSynchronize(C.stream), "batch read");
+  const std::vector<JobSpec>& sp = b->b.specs;
+  const uint32_t nj = b->b.njobs;
+  // one copy per run of jobs whose outputs of this kind lie back to back on
+  // the device (all of them when the batch owns its outputs)
+  auto read = [&](char* host, size_t bpp, auto dev_of, const char* what) -> int {
+    if (!host) return VFR_OK;
+    size_t off = 0;
+    for (uint32_t j = 0; j < nj;) {
+      const char* d0 = (const char*)dev_of(sp[j]);
+      size_t bytes = 0, h0 = off;
+      uint32_t k = j;
+      for (; k < nj; ++k) {
+        const char* d = (const char*)dev_of(sp[k]);
+        const size_t nb = bpp * sp[k].W * sp[k].H;
+        if (!d0 || d != d0 + bytes) break;
+        bytes += nb;
+      }
+      if (k == j) {  // no device output of this kind for job j: skipped
+        off += bpp * sp[j].W * sp[j].H;
+        ++j;
+        continue;
+      }
+      int rc = C.cuda(cudaMemcpyAsync(host + h0, d0, bytes, cudaMemcpyDeviceToHost, b->b.st()), what);
+      if (rc) return rc;
+      off += bytes;
+      j = k;
+    }
+    return VFR_OK;
+  };
+  int rc = read((char*)rgb8_host, 3, [](const JobSpec& q) { return (const void*)q.rgb8; }, "rgb8 read");
+  if (!rc)
+    rc = read((char*)rgba_host, sizeof(float4), [](const JobSpec& q) { return (const void*)q.rgba; },
+              "rgba read");
+  if (!rc)
+    rc = read((char*)steps_host, sizeof(uint32_t),
+              [](const JobSpec& q) { return (const void*)q.steps; }, "steps read");
+  if (!rc) rc = C.cuda(cudaStreamSynchronize(b->b.st()), "batch read");
   return rc;
 }
 

@@ -11,14 +11,21 @@
 //
 // g_scratch is a file-scope __device__ array, so every GPU that loads this
 // library holds kStaticScratchBytes of it until the process exits.  Host code
-// may not use its name as an address: the first call on each device, with
-// that device current, looks its address up with cudaGetSymbolAddress (so
-// make that first call before any stream capture).  All calls share it and
-// it keeps the last call's contents; calls that overlap on the GPU race.
+// may not use its name as an address.  Its device address belongs to a CUDA
+// context (a host application may make its own driver-API context current,
+// and a device reset makes a new one), so every call whose stream is not
+// capturing looks it up again with cudaGetSymbolAddress in the current
+// context and remembers it for that context; a call under stream capture
+// uses the address remembered for its context and is refused if there is
+// none.  All calls share the array and it keeps the last call's contents;
+// calls that overlap on the GPU race.
+#include <cuda.h>  // driver types only: the two context queries come through the runtime
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "vfr_device.cuh"
 #include "vfray.h"
@@ -32,10 +39,11 @@ constexpr size_t kStaticScratchBytes = kPlaneBytes + kCountBytes;
 
 static __device__ __align__(256) unsigned char g_scratch[kStaticScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::once_flag g_once[kMaxDevices];
-void* g_addr[kMaxDevices];
-cudaError_t g_err[kMaxDevices];
+// Addresses of g_scratch found so far, per context (by the context's unique
+// id, which is not reused after a context is destroyed).  Failed lookups are
+// not remembered.
+std::mutex g_mu;
+std::vector<std::pair<unsigned long long, void*>> g_addr;
 
 // Plane coefficients and back-face test of every external face, as
 // vfRayKernelCPU.cc:51-132, and the count of visible faces per block.
@@ -113,14 +121,55 @@ __global__ void __launch_bounds__(kStaticBlock)
   if (vis) vis_ext[s_base + s_warp[warp] + __popc(m & ((1u << lane) - 1u))] = e;
 }
 
-// Address of g_scratch on the current device, looked up once per device.
-cudaError_t scratch_address(int dev, void** out) {
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::call_once(g_once[dev], [dev] {
-    g_err[dev] = cudaGetSymbolAddress(&g_addr[dev], g_scratch);
+// Unique id of the current CUDA context (cuCtxGetCurrent + cuCtxGetId,
+// reached through the runtime's driver entry points, so the library needs no
+// link to the driver library).  False when there is none or the query fails.
+bool current_context_id(unsigned long long* id) {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      get_current = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      get_id = nullptr;
+    cudaGetLastError();
   });
-  *out = g_addr[dev];
-  return g_err[dev];
+  CUcontext c = nullptr;
+  if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c) return false;
+  return get_id(c, id) == CUDA_SUCCESS;
+}
+
+// Address of g_scratch in the current context.  capturing: the stream is
+// under capture, so use the address an earlier call found in this context
+// (VFR_ERR_STATE without one); otherwise look it up now and remember it.
+int scratch_address(bool capturing, void** out) {
+  unsigned long long id = 0;
+  if (!current_context_id(&id)) return VFR_ERR_CUDA;
+  std::lock_guard<std::mutex> g(g_mu);
+  auto it = g_addr.begin();
+  while (it != g_addr.end() && it->first != id) ++it;
+  if (capturing) {
+    if (it == g_addr.end()) return VFR_ERR_STATE;
+    *out = it->second;
+    return VFR_OK;
+  }
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) {
+    cudaGetLastError();
+    return VFR_ERR_CUDA;
+  }
+  if (it != g_addr.end()) it->second = p;
+  else g_addr.emplace_back(id, p);
+  *out = p;
+  return VFR_OK;
 }
 
 bool aligned(const void* p, size_t a) { return ((uintptr_t)p % a) == 0; }
@@ -134,13 +183,18 @@ extern "C" int vfr_find_visible_static(const float* vert4_dev, uint32_t nV, cons
       nT == 0)
     return VFR_ERR_INVALID;
   if (nExt > VFR_STATIC_MAX_EXT) return VFR_ERR_BUDGET;  // beyond the fixed scratch
-  if (!aligned(vert4_dev, 16) || !aligned(tet4_dev, 16) || !aligned(extf2_dev, 8))
+  if (!aligned(vert4_dev, 16) || !aligned(tet4_dev, 16) || !aligned(extf2_dev, 8) ||
+      !aligned(visExt_dev, 4) || !aligned(num_vis_dev, 4))
     return VFR_ERR_INVALID;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return VFR_ERR_CUDA;
-  void* scratch = nullptr;
-  if (scratch_address(dev, &scratch) != cudaSuccess || !scratch) return VFR_ERR_CUDA;
   cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return VFR_ERR_CUDA;
+  }
+  void* scratch = nullptr;
+  const int rc = scratch_address(cs != cudaStreamCaptureStatusNone, &scratch);
+  if (rc) return rc;
   if (cudaMemsetAsync(num_vis_dev, 0, sizeof(uint32_t), s) != cudaSuccess) return VFR_ERR_CUDA;
   if (nExt) {
     const uint32_t nblk = (nExt + kStaticBlock - 1) / kStaticBlock;

@@ -76,12 +76,29 @@ struct SharedTables {
   double e2[64];
 };
 
+// A ray's walk is a function of its state (tet, entry face) alone: the pixel
+// is fixed, so a state that comes back means the reference's while loop
+// never ends (a cycle among tets around a projected edge, which the
+// inclusive exit tests with slack allow on meshes whose tets list their
+// vertices in arbitrary order).  Rays longer than kWatchSteps iterations are
+// watched: the state is saved at every power-of-two iteration count and
+// compared with the state of every later iteration (Brent), which stops a
+// cycling ray within about two periods.  Shorter rays pay one comparison
+// per step.  The oracle applies the same rule, so steps stay comparable.
+constexpr uint32_t kWatchSteps = 4095;
+
+// The watched state of each thread's ray (tet << 2 | entry face, ~0 =
+// none), in shared memory: it is written when a segment starts and read
+// only by watched iterations, so it takes no register of the step.
+__shared__ uint32_t s_watch_saved[256];
+
 struct Ray {
   float4 r0, r1, r2, r3;       // vertices rotated by the entry face
   WalkRec w;                   // walk record of the current tet
   const WalkRec* walk;         // this job's mesh and view vertices
   const float4* vert;
-  uint32_t j, nT, cap;
+  uint32_t j, nT;
+  uint32_t watch;              // min(kWatchSteps, step cap): longer rays are checked
   double rmaxEdge;             // 1 / maxEdgeLength, correctly rounded (div_by)
   uint32_t cbi;                // colorBack: its transfer-function entry
   uint32_t t, f, p, iters;
@@ -117,6 +134,7 @@ __device__ __forceinline__ void begin_segment(const JobDev& J, Ray& R, uint32_t 
   R.zp = zp;
   R.lastZ = zp;
   R.cbi = (uint32_t)fmul(255.0f, sp);
+  s_watch_saved[threadIdx.x] = 0xffffffffu;  // a new segment walks other states
 }
 
 // Composited mode: the next entry of the pixel in (depth, index) descending
@@ -165,7 +183,25 @@ __device__ __forceinline__ void finish_pixel(const JobDev& J, const Ray& R) {
   if (J.steps) J.steps[R.p] = R.iters;
 }
 
-enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kAbandon = 2, kCap = 3, kRange = 4 };
+enum StepResult : uint32_t { kContinue = 0, kSegmentEnd = 1, kCycle = 2, kCap = 3, kRange = 4 };
+
+// The step cap of a ray of this job: the option, or 4 nT + 64 (a walk that
+// repeats no state has at most 4 nT iterations).
+__device__ __forceinline__ uint32_t step_cap_of(const TraverseParams& P, uint32_t nT) {
+  return P.step_cap ? P.step_cap : min(4u * nT + 64u, 0x7fffffffu);
+}
+
+// Rare: an iteration beyond the watch threshold.  The cap, then Brent's
+// check of the state this iteration starts from (R.t, R.f are still the
+// current tet and entry face).
+__device__ __forceinline__ uint32_t watched_step(const TraverseParams& P, Ray& R) {
+  if (R.iters > step_cap_of(P, R.nT)) return kCap;
+  const uint32_t key = (R.t << 2) | R.f;  // nT < 2^30 (checked at upload)
+  uint32_t& saved = s_watch_saved[threadIdx.x];
+  if (key == saved) return kCycle;
+  if ((R.iters & (R.iters - 1u)) == 0u) saved = key;
+  return kContinue;
+}
 
 // The step's depth difference and extinctions from the exit face's depth zn
 // and scalar sn at the pixel (:437-457): dz = |zPrev - zNext| (0 below
@@ -237,15 +273,19 @@ __device__ __forceinline__ StepColour composite(const TraverseParams& P, const S
 }
 
 // One iteration of the reference's while loop (:302-542).  The ways it can
-// end before compositing (step cap, no exit face, id range, scalar or psi
-// coordinate out of range) are folded into a status and the arithmetic runs
+// end before compositing (a cycle or the step cap, no exit face, id range,
+// scalar or psi coordinate out of range) are folded into a status and the
+// arithmetic runs
 // on for every lane; the colour is only committed while the status says to
 // go on, so no lane takes an early branch.  The exact fallbacks of the
 // plane, zeta and the psi coordinates are gathered into one rare block
 // after the fast path, so the step from the exit tests to the advance is
 // one straight run of code that the compiler schedules as a whole.
 __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTables& S, Ray& R) {
-  uint32_t st = (++R.iters > R.cap) ? kCap : kContinue;
+  // rare: an iteration of a long ray is watched for a cycle (its verdict
+  // ends the step like the cap: nothing of it is committed)
+  uint32_t st = kContinue;
+  if (++R.iters > R.watch) st = watched_step(P, R);
   const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
   const bool h3 = exit_test(R.r3, R.r0, R.r1, R.ox, R.oy);
@@ -400,7 +440,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
           R.walk = J.walk;
           R.vert = J.vert;
           R.nT = J.nT;
-          R.cap = P.step_cap ? P.step_cap : min(4u * J.nT + 64u, 0x7fffffffu);
+          R.watch = min(kWatchSteps, step_cap_of(P, J.nT));
           R.rmaxEdge = __drcp_rn((double)job_maxedge(J));
           R.p = J.rays[g - P.ray_pref[j]];
           const uint32_t x = R.p % J.W, y = R.p / J.W;
@@ -448,10 +488,9 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
         if (next_entry(P, P.jobs[R.j], R, false)) continue;
       }
       finish_pixel(P.jobs[R.j], R);
-    } else if (res == kAbandon) {
-      T.status |= 1u;  // the reference writes nothing for this pixel (:365)
-    } else if (res == kCap) {
-      T.status |= 2u;
+    } else if (res == kCycle || res == kCap) {
+      // the pixel keeps what the ray composited before it was stopped
+      T.status |= res == kCycle ? 32u : 2u;  // VFR_DEV_CYCLE, VFR_DEV_STEP_CAP
       finish_pixel(P.jobs[R.j], R);
     } else {
       T.status |= 4u;

@@ -9,7 +9,8 @@
 //
 // Options (all optional, before the volume name): --dir DIR (dataset
 // directory, default ../tet_offs/), --size WxH, --psi FILE (a
-// psiGammaTable512.h-style table; default: the library's generated table),
+// psiGammaTable512.h-style table, or "generated" for the table this library
+// computes; default: the reference's own table, vfr_psi_table_reference),
 // --mode ref|composited, --device N, --out FILE.ppm, --rgba FILE (raw
 // float32 RGBA), --steps FILE (raw uint32 steps per pixel), --cache (read
 // the normalised mesh, conTet, external faces and limits from <volume>.vfrb
@@ -205,13 +206,19 @@ int main(int argc, char** argv) {
   std::printf("  Max Z: %f ; Min Z: %f\n", lmt[1], lmt[2]);
 
   std::vector<float> psi(512 * 512);
-  if (!psi_path.empty()) {
+  if (psi_path == "generated") {
+    vfr_psi_table(psi.data());
+    std::printf("psi table: generated\n");
+  } else if (!psi_path.empty()) {
     if ((rc = vfr_read_psi_source(psi_path.c_str(), psi.data())) != VFR_OK)
       return die(("reading psi table " + psi_path).c_str(), rc);
     std::printf("psi table: %s\n", psi_path.c_str());
   } else {
-    vfr_psi_table(psi.data());
-    std::printf("psi table: generated\n");
+    if ((rc = vfr_psi_table_reference(psi.data())) != VFR_OK)
+      return die("the reference psi table (data/psiGammaTable512.bin beside the library) is "
+                 "missing; use --psi FILE or --psi generated",
+                 rc);
+    std::printf("psi table: the reference's (psiGammaTable512.h)\n");
   }
 
   // --- device (vfRay.cu:885-911) ---
