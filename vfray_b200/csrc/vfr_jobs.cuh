@@ -34,7 +34,7 @@ __global__ void init_jobs_kernel(const JobDev* __restrict__ jobs, uint32_t njobs
   if (j >= njobs) return;
   ViewCounters v;
   v.nvis = 0; v.nrays = 0; v.nentries = 0; v.status = 0; v.steps = 0;
-  v.maxedge_bits = 0; v.pad = 0;
+  v.maxedge_bits = 0; v.rays_done = 0;
   for (int k = 0; k < 4; ++k) { v.mm[k] = 0xffffffffu; v.mm[4 + k] = 0u; }
   *jobs[j].ctr = v;
 }

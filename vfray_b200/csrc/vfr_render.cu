@@ -308,6 +308,9 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     J.ent_off = mode == VFR_MODE_COMPOSITED ? ent_off.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
     J.ent_cur = mode == VFR_MODE_COMPOSITED ? ent_cur.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
     J.ctr = d_ctr.as<ViewCounters>(sizeof(ViewCounters) * j);
+    J.ent = mode == VFR_MODE_COMPOSITED ? ent.as<uint2>() : nullptr;
+    J.ent_cap = (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu);
+    J.mode = (uint32_t)mode;
     if (own_outputs) {
       specs[j].rgb8 = out_rgb8.as<uint8_t>(3 * op);
       specs[j].rgba = out_rgba.as<float4>(sizeof(float4) * op);
@@ -421,8 +424,6 @@ int Batch::enqueue_c() {
   P.njobs = njobs;
   P.ray_pref = ray_pref();
   P.queue = queue();
-  P.ent = mode == VFR_MODE_COMPOSITED ? ent.as<uint2>() : nullptr;
-  P.ent_cap = (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu);
   P.tf = C.d_tf;
   P.psi = C.d_psi;
   P.e2tab = reinterpret_cast<const double*>(C.d_tf + 256);

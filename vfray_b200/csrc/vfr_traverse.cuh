@@ -84,7 +84,8 @@ struct SharedTables {
 // watched: the state is saved at every power-of-two iteration count and
 // compared with the state of every later iteration (Brent), which stops a
 // cycling ray within about two periods.  Shorter rays pay one comparison
-// per step.  The oracle applies the same rule, so steps stay comparable.
+// per pass of two steps.  The oracle applies the same rule, so steps stay
+// comparable.
 constexpr uint32_t kWatchSteps = 4095;
 
 // The watched state of each thread's ray (tet << 2 | entry face, ~0 =
@@ -107,6 +108,10 @@ struct Ray {
   // composited mode: this pixel's entry list and the last entry taken
   uint32_t ea, en, dz_bits, de;
   float exitZ;
+  // served form: the job (its table entry lives in the server's arena) and
+  // its completion flag
+  const JobDev* jp;
+  uint32_t* done;
 };
 
 // Read-only loads of the mesh through the non-coherent path (the arrays are
@@ -148,7 +153,7 @@ __device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev
     bool found = false;
     const float dzl = __uint_as_float(R.dz_bits);
     for (uint32_t k = 0; k < R.en; ++k) {
-      const uint2 q = P.ent[R.ea + k];
+      const uint2 q = J.ent[R.ea + k];
       const float z = __uint_as_float(q.x);
       const bool below = first || (z < dzl) || (z == dzl && q.y < R.de);
       if (!below) continue;
@@ -281,11 +286,16 @@ __device__ __forceinline__ StepColour composite(const TraverseParams& P, const S
 // plane, zeta and the psi coordinates are gathered into one rare block
 // after the fast path, so the step from the exit tests to the advance is
 // one straight run of code that the compiler schedules as a whole.
+//
+// kWatched: the iteration is past the watch threshold and checked for a
+// cycle first (its verdict ends the step like the cap: nothing of it is
+// committed).  The loop below takes the unwatched form, which carries no
+// trace of the check, for every pass that stays below the threshold.
+template <bool kWatched, bool kServe = false>
 __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTables& S, Ray& R) {
-  // rare: an iteration of a long ray is watched for a cycle (its verdict
-  // ends the step like the cap: nothing of it is committed)
+  ++R.iters;
   uint32_t st = kContinue;
-  if (++R.iters > R.watch) st = watched_step(P, R);
+  if (kWatched) st = watched_step(P, R);
   const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
   const bool h3 = exit_test(R.r3, R.r0, R.r1, R.ox, R.oy);
@@ -368,7 +378,7 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   }
   if (st == kContinue && code >= 6) {
     // shared face not matched by vertex ids: reload the tet's vertices
-    const uint4 id = __ldg(P.jobs[R.j].tet + tn);
+    const uint4 id = __ldg((kServe ? R.jp->tet : P.jobs[R.j].tet) + tn);
     R.r0 = __ldg(R.vert + sel4(id, fn));
     R.r1 = __ldg(R.vert + sel4(id, (fn + 1) & 3u));
     R.r2 = __ldg(R.vert + sel4(id, (fn + 2) & 3u));
@@ -379,6 +389,50 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   R.f = fn;
   R.zp = zn;
   return st;
+}
+
+// Start the ray of the job's local ray index `local`: its pixel, the
+// pixel's object coordinates, and its first segment -- the winning entry
+// face (reference mode) or the first entry of the pixel's list (composited
+// mode; kMode 2 takes the mode from the job).  Returns whether the ray
+// walks; a composited pixel without a usable entry is finished here.
+template <int kMode>
+__device__ __forceinline__ bool start_ray(const TraverseParams& P, const JobDev& J, Ray& R,
+                                          uint32_t local, uint32_t& status) {
+  R.walk = J.walk;
+  R.vert = J.vert;
+  R.nT = J.nT;
+  R.watch = min(kWatchSteps, step_cap_of(P, J.nT));
+  R.rmaxEdge = __drcp_rn((double)job_maxedge(J));
+  R.p = J.rays[local];
+  const uint32_t x = R.p % J.W, y = R.p / J.W;
+  R.ox = obj_coord(x, J.W);
+  R.oy = obj_coord(y, J.H);
+  R.ar = R.ag = R.ab = 0.0f;
+  R.tr = 1.0f;
+  R.iters = 0;
+  const bool ref = kMode == 0 || (kMode == 2 && J.mode == 0);
+  if (ref) {
+    const uint32_t e = (uint32_t)J.winner[R.p];
+    const float4 p0 = J.planes[kPlaneStride * (size_t)e];
+    const float4 p1 = J.planes[kPlaneStride * (size_t)e + 1];
+    begin_segment(J, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
+                  plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
+    return true;
+  }
+  R.ea = J.ent_off[R.p];
+  const uint32_t b1 = J.ent_off[R.p + 1];
+  R.en = b1 - R.ea;
+  R.exitZ = INFINITY;
+  R.dz_bits = 0;
+  R.de = 0;
+  if (b1 > J.ent_cap) {
+    status |= 16u;  // VFR_DEV_OVERFLOW: the caller renders again with room
+    return false;
+  }
+  if (next_entry(P, J, R, true)) return true;
+  finish_pixel(J, R);
+  return false;
 }
 
 // Per-lane tallies of tet-walk steps and status bits, flushed to the job's
@@ -401,9 +455,7 @@ __device__ __forceinline__ void flush(const TraverseParams& P, Tally& T) {
 
 // kMinBlocks: CTAs of 256 threads the register budget must allow per SM
 // (2: no spills; 3: 80 registers, a few spilled to L1).
-template <int kMode, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParams P) {
-  __shared__ SharedTables S;
+__device__ __forceinline__ void load_tables(const TraverseParams& P, SharedTables& S) {
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
     const float4 c = P.tf[i];
     S.rg[i] = make_double2((double)c.x, (double)c.y);
@@ -412,6 +464,12 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
   }
   for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) S.e2[i] = P.e2tab[i];
   __syncthreads();
+}
+
+template <int kMode, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParams P) {
+  __shared__ SharedTables S;
+  load_tables(P, S);
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt_mask = (1u << lane) - 1u;
   const uint32_t nrays = P.ray_pref[P.njobs];
@@ -437,39 +495,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
             T.j = j;
           }
           R.j = j;
-          R.walk = J.walk;
-          R.vert = J.vert;
-          R.nT = J.nT;
-          R.watch = min(kWatchSteps, step_cap_of(P, J.nT));
-          R.rmaxEdge = __drcp_rn((double)job_maxedge(J));
-          R.p = J.rays[g - P.ray_pref[j]];
-          const uint32_t x = R.p % J.W, y = R.p / J.W;
-          R.ox = obj_coord(x, J.W);
-          R.oy = obj_coord(y, J.H);
-          R.ar = R.ag = R.ab = 0.0f;
-          R.tr = 1.0f;
-          R.iters = 0;
-          if (kMode == 0) {
-            const uint32_t e = (uint32_t)J.winner[R.p];
-            const float4 p0 = J.planes[kPlaneStride * (size_t)e];
-            const float4 p1 = J.planes[kPlaneStride * (size_t)e + 1];
-            begin_segment(J, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
-                          plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
-            active = true;
-          } else {
-            R.ea = J.ent_off[R.p];
-            const uint32_t b1 = J.ent_off[R.p + 1];
-            R.en = b1 - R.ea;
-            R.exitZ = INFINITY;
-            R.dz_bits = 0;
-            R.de = 0;
-            if (b1 > P.ent_cap) {
-              T.status |= 16u;  // VFR_DEV_OVERFLOW: the caller renders again with room
-            } else {
-              active = next_entry(P, J, R, true);
-              if (!active) finish_pixel(J, R);
-            }
-          }
+          active = start_ray<kMode>(P, J, R, g - P.ray_pref[j], T.status);
         }
       }
     }
@@ -478,9 +504,16 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
       continue;
     }
     if (!active) continue;
-    // two steps per pass of the loop: the refill test runs half as often
-    uint32_t res = step(P, S, R);
-    if (res == kContinue) res = step(P, S, R);
+    // two steps per pass of the loop: the refill test runs half as often.
+    // A pass that would reach the watch threshold takes one watched step
+    // instead (rare: rays longer than kWatchSteps iterations).
+    uint32_t res;
+    if (R.iters + 2u <= R.watch) {
+      res = step<false>(P, S, R);
+      if (res == kContinue) res = step<false>(P, S, R);
+    } else {
+      res = step<true>(P, S, R);
+    }
     if (res == kContinue) continue;
     if (res == kSegmentEnd) {
       if (kMode == 1) {
@@ -499,6 +532,156 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
     active = false;
   }
   flush(P, T);
+}
+
+// ---------------------------------------------------------------- served
+
+// A served ray has ended: its steps and status go to its job's counters,
+// then its count of finished rays; the lane that finishes the job's last ray
+// sets the job's completion flag in mapped host memory.  Each lane's pixel
+// and counter writes are fenced before its count, and the last lane fences
+// at system scope before the flag, so everything the job wrote is visible
+// to the host's copy once the flag is.
+__device__ __forceinline__ void served_ray_done(const Ray& R, uint32_t status) {
+  ViewCounters* c = R.jp->ctr;
+  atomicAdd(&c->steps, (unsigned long long)R.iters);
+  if (status) atomicOr(&c->status, status);
+  __threadfence();
+  const uint32_t n = atomicAdd(&c->rays_done, 1u) + 1u;
+  if (n == *(volatile const uint32_t*)&c->nrays) {
+    __threadfence_system();
+    *(volatile uint32_t*)R.done = 1u;
+  }
+}
+
+// The served form's persistent traversal: one long-lived launch whose warps
+// take rays from the published segments in order, oldest first, while the
+// host publishes new ones (requests admitted while this launch runs fold
+// into it).  A warp holds its place in the segment table: it takes rays from
+// its current entry with one atomicAdd on the entry's head and moves on once
+// the entry is drained.  Jobs of either mode may be mixed (kMode 2 per job).
+// A warp with nothing to do polls for newly published segments: it leaves
+// when the host's stop flag is set, or sets VFR_DEV_QUEUE in the control
+// word and leaves when idle_limit polls found nothing -- a bounded wait, so
+// a launch never outlives its work by more than about idle_limit
+// microseconds.  The host relaunches it when work arrives after it left.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) serve_kernel(ServeParams SP) {
+  const TraverseParams& P = SP.T;
+  __shared__ SharedTables S;
+  load_tables(P, S);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const uint32_t refill = P.refill ? P.refill : 1u;
+  uint32_t cur = SP.ctl->first;  // this warp's entry of the segment table
+  uint32_t idle_polls = 0;
+  bool active = false;
+  Ray R;
+  for (;;) {
+    const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+    uint32_t seg = 0xffffffffu;
+    if (idle && ((uint32_t)__popc(idle) >= refill || idle == 0xffffffffu)) {
+      const uint32_t leader = __ffs(idle) - 1u, k = __popc(idle);
+      uint32_t base = 0, nr = 0;
+      if (lane == leader) {
+        uint32_t pub;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(pub) : "l"(&SP.ctl->published));
+        while (cur < pub) {
+          SegDev* sg = SP.segs + cur;
+          const uint32_t b = atomicAdd(&sg->head, k);
+          const uint32_t n = sg->nrays;  // written before the entry was published
+          if (b < n) {
+            base = b;
+            nr = n;
+            seg = cur;
+            break;
+          }
+          ++cur;  // drained: the next entry
+        }
+      }
+      cur = __shfl_sync(0xffffffffu, cur, leader);
+      seg = __shfl_sync(0xffffffffu, seg, leader);
+      base = __shfl_sync(0xffffffffu, base, leader);
+      nr = __shfl_sync(0xffffffffu, nr, leader);
+      if (seg != 0xffffffffu && !active) {
+        const uint32_t g = base + __popc(idle & lt_mask);
+        if (g < nr) {
+          const SegDev& sg = SP.segs[seg];
+          const uint32_t j = job_of(sg.ray_pref, sg.njobs, g);
+          R.jp = sg.jobs + j;
+          R.done = sg.done + j;
+          uint32_t status = 0;
+          active = start_ray<2>(P, *R.jp, R, g - sg.ray_pref[j], status);
+          if (!active) served_ray_done(R, status);
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (seg == 0xffffffffu) {  // nothing published to take: wait, boundedly
+        if (*SP.stop) break;
+        if (++idle_polls > SP.idle_limit) {
+          if (lane == 0) atomicOr(&SP.ctl->status, 8u);  // VFR_DEV_QUEUE
+          break;
+        }
+        __nanosleep(1000);
+      }
+      continue;
+    }
+    idle_polls = 0;
+    if (!active) continue;
+    uint32_t res;
+    if (R.iters + 2u <= R.watch) {
+      res = step<false, true>(P, S, R);
+      if (res == kContinue) res = step<false, true>(P, S, R);
+    } else {
+      res = step<true, true>(P, S, R);
+    }
+    if (res == kContinue) continue;
+    uint32_t status = 0;
+    if (res == kSegmentEnd) {
+      if (R.jp->mode == 1) {
+        R.exitZ = R.lastZ;
+        if (next_entry(P, *R.jp, R, false)) continue;
+      }
+      finish_pixel(*R.jp, R);
+    } else if (res == kCycle || res == kCap) {
+      status = res == kCycle ? 32u : 2u;
+      finish_pixel(*R.jp, R);
+    } else {
+      status = 4u;
+    }
+    served_ray_done(R, status);
+    active = false;
+  }
+}
+
+// Publishes a prepared segment: its table entry, then (release) the count
+// of published entries the served launch acquires.  Jobs without rays are
+// complete now: their pixels were cleared by stage (b).
+__global__ void publish_kernel(SegDev* segs, ServeCtl* ctl, uint32_t seq, const JobDev* jobs,
+                               const uint32_t* ray_pref, uint32_t* done, uint32_t njobs) {
+  if (threadIdx.x == 0) {
+    SegDev d;
+    d.jobs = jobs;
+    d.ray_pref = ray_pref;
+    d.done = done;
+    d.njobs = njobs;
+    d.nrays = ray_pref[njobs];
+    d.head = 0;
+    d.pad = 0;
+    segs[seq] = d;
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < njobs; j += blockDim.x)
+    if (ray_pref[j + 1] == ray_pref[j]) {
+      __threadfence_system();
+      *(volatile uint32_t*)(done + j) = 1u;
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&ctl->published), "r"(seq + 1u) : "memory");
+  }
 }
 
 }  // namespace vfr

@@ -13,7 +13,7 @@ struct __align__(16) ViewCounters {
   uint32_t status;           // VFR_DEV_* bits
   unsigned long long steps;  // tet-walk iterations of this job's rays
   uint32_t maxedge_bits;     // view maxEdgeLength (float bits, >= 0)
-  uint32_t pad;
+  uint32_t rays_done;        // served form: rays of this job finished so far
   uint32_t mm[8];            // orderable min x y z s, max x y z s (view set-up)
 };
 
@@ -37,6 +37,8 @@ struct __align__(16) JobDev {
   uint32_t* ent_cnt;         // composited: W*H counts (batch arena)
   uint32_t* ent_off;         // composited: offsets (batch arena, global)
   uint32_t* ent_cur;
+  const uint2* ent;          // composited: the batch's entry arena (z bits, ext face)
+  uint32_t ent_cap;          // its capacity in entries
   ViewCounters* ctr;
   uint8_t* rgb8;             // outputs (any may be null)
   float4* rgba;
@@ -45,6 +47,7 @@ struct __align__(16) JobDev {
   uint32_t use_mv;
   float maxEdge_in;          // the mesh's maxEdgeLength when !use_mv
   uint32_t pix_base;         // first pixel of this job in the batch's pixel arenas
+  uint32_t mode;             // VFR_MODE_REF or VFR_MODE_COMPOSITED
 };
 
 // Face planes per external face: three float4, (zx zy zz sx | sy sz v0x v0y |
@@ -57,13 +60,46 @@ struct TraverseParams {
   uint32_t njobs;
   const uint32_t* ray_pref;  // njobs + 1, exclusive prefix of the jobs' ray counts
   uint32_t* queue;           // work-queue head over all jobs' rays
-  const uint2* ent;          // composited: entry arena (z bits, ext face)
-  uint32_t ent_cap;
   const float4* tf;          // 256 RGBA
   const float* psi;          // 512 x 512
   const double* e2tab;       // 2^(j/64), j = 0..63
   uint32_t step_cap;         // 0: 4 * nT + 64 of each job's mesh
   uint32_t refill;           // refill a warp's idle lanes once this many are idle
+};
+
+// ---- served form ----
+//
+// One long-lived persistent traversal launch draws rays from segments: each
+// admitted mini-batch of render jobs, laid out in the server's arena, is
+// prepared (stages a and b) on another stream while the launch runs and then
+// published into the next entry of the segment table.  Within one launch an
+// entry, and the arena memory its jobs use, is written once before its
+// publication and never reused; the server starts a new epoch (table and
+// arena from the start) only between launches.
+
+struct SegDev {
+  const JobDev* jobs;        // the segment's job table
+  const uint32_t* ray_pref;  // njobs + 1, exclusive prefix of its jobs' ray counts
+  uint32_t* done;            // per job, mapped host memory: set to 1 when its last ray ends
+  uint32_t njobs;
+  uint32_t nrays;            // ray_pref[njobs]
+  uint32_t head;             // rays handed out so far (atomicAdd; may pass nrays)
+  uint32_t pad;
+};
+
+struct ServeCtl {
+  uint32_t published;        // entries of the segment table published in this epoch
+  uint32_t status;           // VFR_DEV_QUEUE: an idle warp's bounded wait gave up
+  uint32_t first;            // the oldest entry with rays left when the launch starts
+  uint32_t pad;
+};
+
+struct ServeParams {
+  TraverseParams T;          // tables, step cap, refill (jobs, ray_pref, queue unused)
+  SegDev* segs;
+  ServeCtl* ctl;
+  const volatile uint32_t* stop;  // mapped host memory: the host asks idle warps to leave
+  uint32_t idle_limit;       // polls (about 1 us each) an idle warp makes before it gives up
 };
 
 }  // namespace vfr

@@ -88,13 +88,22 @@ def carve(xyz: np.ndarray, tets: np.ndarray, seed: int, count: int = 16,
     """Drop tets whose centroid value of a seeded Gaussian field exceeds the
     given percentile; drop and re-index unreferenced vertices (vertex and tet
     order are otherwise preserved)."""
-    # centroid field in chunks (the same values; bounded temporaries for
-    # meshes of 10^8 tets)
+    # centroid field in chunks on a thread pool (numpy's array operations
+    # release the interpreter lock; each chunk does the same operations on
+    # its elements, so the values do not depend on the chunking or the
+    # threads), with bounded temporaries for meshes of 10^8 tets
+    from concurrent.futures import ThreadPoolExecutor
+    import os
+
     val = np.empty(tets.shape[0], dtype=np.float64)
-    step = 1 << 22
-    for lo in range(0, tets.shape[0], step):
+    step = 1 << 20
+
+    def chunk(lo):
         cen = xyz[tets[lo:lo + step]].mean(axis=1)
         val[lo:lo + step] = gaussian_field(cen, count, seed)
+
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+        list(ex.map(chunk, range(0, tets.shape[0], step)))
     keep = val <= np.percentile(val, percentile)
     tets = tets[keep]
     used = np.zeros(xyz.shape[0], dtype=bool)
