@@ -230,14 +230,23 @@ VFR_API int vfr_batch_scratch_bytes(vfr_batch* b, uint64_t* bytes);
 /* ---- served form: a request loop with continuous batching -------------- */
 
 /* No counterpart in the reference.  Requests over the context's resident
- * meshes are submitted from any thread; a worker thread admits them in
- * arrival order while their memory footprint (the view's scratch and image
- * buffers) fits the budget left, folds all admitted requests -- meshes and
- * image sizes mixed -- into one batch and launches it on one of two batch
- * slots with their own streams, so a batch formed while another runs
- * overlaps it on the device.  A request whose footprint exceeds the whole
- * budget is refused (VFR_ERR_BUDGET).  Upload the meshes before creating the
- * server and release them after destroying it. */
+ * meshes are submitted from any thread.  One long-lived persistent
+ * traversal launch (the drain) takes rays from every request admitted so
+ * far: a worker thread admits pending requests in arrival order while their
+ * memory footprint fits the budget, prepares them (stages a and b) on a
+ * second stream beside the running drain, and publishes them into its work
+ * table, so requests that arrive while others are on the GPU fold into the
+ * running launch, frames of any size mixed.  When a request's last ray
+ * ends, its image is copied to rgb8_host and its footprint released.
+ * The budget covers the resident meshes of the context (counted once) and,
+ * per request in flight, its view's scratch (view vertices, planes, visible
+ * list, boxes, winner map or entry lists, ray list) and RGB8 image; the
+ * server allocates that as one arena when it starts and nothing afterwards.
+ * A request whose footprint can never fit is refused (VFR_ERR_BUDGET).
+ * Upload the meshes before creating the server and release them after
+ * destroying it; while the drain runs, calls on the same context that free
+ * or grow device memory wait until it goes idle (about 50 ms after the last
+ * request). */
 typedef struct {
   int mesh_id;
   uint32_t W, H;
@@ -249,15 +258,22 @@ typedef struct {
 
 typedef struct {
   int status;
-  double t_submit_ms, t_start_ms, t_done_ms;  /* since the server started */
-  uint32_t batch_id, batch_jobs;               /* the batch it ran in, its size */
+  double t_submit_ms, t_start_ms, t_done_ms;  /* since the server started; start = admission */
+  uint32_t batch_id, batch_jobs;               /* the admitted group it joined, its size */
   uint32_t num_rays;
   uint64_t num_steps;
+  uint32_t device_status;                      /* VFR_DEV_* bits of its job */
 } vfr_request_info;
 
 typedef struct {
-  uint32_t batches, pending;
+  uint32_t batches, pending;                   /* admitted groups so far; requests waiting */
   uint64_t completed, rejected, budget_used, rays, steps;
+  uint32_t launches;        /* drain launches (a new one after each idle period) */
+  uint32_t epochs;          /* arena restarts */
+  uint32_t queue_timeouts;  /* drain launches whose bounded idle wait ran out (VFR_DEV_QUEUE) */
+  uint64_t mesh_bytes;      /* resident mesh bytes counted against the budget */
+  uint64_t arena_bytes;     /* the arena for requests in flight */
+  double prep_ms;           /* device time of the finished groups' preparation (stages a, b) */
 } vfr_server_counters;
 
 typedef struct vfr_server vfr_server;
@@ -268,6 +284,12 @@ VFR_API int vfr_server_submit(vfr_server* s, const vfr_request* r, uint64_t* tic
  * out), fills info, forgets the ticket; returns the request's status. */
 VFR_API int vfr_server_wait(vfr_server* s, uint64_t ticket, int timeout_ms, vfr_request_info* info);
 VFR_API int vfr_server_stats(vfr_server* s, vfr_server_counters* out);
+/* Idle behaviour: the drain's bounded wait for new work (polls of about a
+ * microsecond each, default 400000; when it runs out the drain sets
+ * VFR_DEV_QUEUE, leaves, and is launched again with the next request) and
+ * how long the worker lets an idle drain run before it stops it and starts
+ * a new arena epoch (default 50 ms).  Applies from the next drain launch. */
+VFR_API int vfr_server_set_idle(vfr_server* s, uint32_t drain_idle_polls, uint32_t linger_ms);
 /* Drains the admitted and pending requests, then stops. */
 VFR_API void vfr_server_destroy(vfr_server* s);
 

@@ -199,3 +199,59 @@ def test_cycling_ray_is_stopped(renderer, oracle_lib):
         renderer.render(mid, 64, 64)
     finally:
         renderer.release_mesh(mid)
+
+
+def test_mixed_workload_full_size_sampled_rays(renderer, oracle_lib):
+    """The uneven-jobs workload at its extremes, in one batch: a 1024^2 view
+    of the carved 128^3 mesh (10.7 M tets) and a 128^2 view of the carved
+    16^3 mesh.  Per job: every pixel's entry face against the oracle's
+    winner pass (through the ray count and the zero/non-zero steps), 4,000
+    seeded rays traced by the oracle (steps bit for bit, colour within
+    tolerance), and the step sum."""
+    tf, psi = synth.transfer_function(2), vb.reference_psi_table()
+    renderer.upload_tables(tf, psi)
+    cases = []
+    for n, res, seed in [(128, 1024, 7), (16, 128, 3)]:
+        vert, tet = synth.make_mesh(n, carved=True, view_seed=None, jitter_seed=7,
+                                    scalar_seed=8, carve_seed=11)
+        p = vb.prepare(vert, tet)
+        mid = renderer.upload_mesh(p["vert"], p["tet"], p["con"], p["extf"], p["lmt"])
+        cases.append((p, mid, res, synth.orbit_views(4, seed=seed)[1]))
+    try:
+        jobs = [(mid, mv, res, res) for (_, mid, res, mv) in cases]
+        B = vbatch.BatchRenderer(renderer, jobs)
+        try:
+            B.prepare()
+            B.run()
+            stats = B.stats()
+            npx = sum(r * r for (_, _, r, _) in cases)
+            rgb = np.empty(npx * 3, np.uint8)
+            rgba = np.empty(npx * 4, np.float32)
+            steps = np.empty(npx, np.uint32)
+            B.read(rgb8=rgb, rgba=rgba, steps=steps)
+        finally:
+            B.close()
+        rng = np.random.default_rng(5)
+        off = 0
+        for j, (p, _, res, mv) in enumerate(cases):
+            n = res * res
+            vv = vb.normalize(vb.rotate(p["vert"], mv))
+            m = oracle_lib.mesh(vv, p["tet"], p["con"], p["extf"], tf, psi,
+                                vb.build_lmt(vv, p["tet"])[0])
+            wr = oracle_lib.winners(m, res, res).ravel()
+            st = steps[off:off + n]
+            rays = np.flatnonzero(wr >= 0)
+            assert stats[j]["num_rays"] == len(rays)
+            assert np.all(st[rays] > 0) and np.all(st[wr < 0] == 0)
+            assert stats[j]["num_steps"] == int(st.sum(dtype=np.uint64))
+            sample = rng.choice(rays, size=min(4000, len(rays)), replace=False).astype(np.uint32)
+            t = oracle_lib.trace_pixels(m, res, res, sample, wr[sample])
+            assert np.array_equal(st[sample], t["steps"])
+            d = np.abs(rgb[3 * off:3 * (off + n)].reshape(-1, 3)[sample].astype(int) - t["rgb8"].astype(int))
+            assert d.max() <= 2
+            rms = np.sqrt(np.mean((rgba[4 * off:4 * (off + n)].reshape(-1, 4)[sample, :3] - t["rgba"][:, :3]) ** 2))
+            assert rms <= 1e-3
+            off += n
+    finally:
+        for (_, mid, _, _) in cases:
+            renderer.release_mesh(mid)

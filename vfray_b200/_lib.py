@@ -85,7 +85,8 @@ class RequestInfo(C.Structure):
     """vfr_request_info of include/vfray.h."""
     _fields_ = [("status", C.c_int), ("t_submit_ms", C.c_double), ("t_start_ms", C.c_double),
                 ("t_done_ms", C.c_double), ("batch_id", C.c_uint32), ("batch_jobs", C.c_uint32),
-                ("num_rays", C.c_uint32), ("num_steps", C.c_uint64)]
+                ("num_rays", C.c_uint32), ("num_steps", C.c_uint64),
+                ("device_status", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -95,7 +96,9 @@ class ServerStats(C.Structure):
     """vfr_server_stats of include/vfray.h."""
     _fields_ = [("batches", C.c_uint32), ("pending", C.c_uint32), ("completed", C.c_uint64),
                 ("rejected", C.c_uint64), ("budget_used", C.c_uint64), ("rays", C.c_uint64),
-                ("steps", C.c_uint64)]
+                ("steps", C.c_uint64), ("launches", C.c_uint32), ("epochs", C.c_uint32),
+                ("queue_timeouts", C.c_uint32), ("mesh_bytes", C.c_uint64),
+                ("arena_bytes", C.c_uint64), ("prep_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -142,6 +145,7 @@ SIGNATURES = {
     "vfr_server_submit": (_i, [_vp, C.POINTER(Request), C.POINTER(C.c_uint64)]),
     "vfr_server_wait": (_i, [_vp, C.c_uint64, _i, C.POINTER(RequestInfo)]),
     "vfr_server_stats": (_i, [_vp, C.POINTER(ServerStats)]),
+    "vfr_server_set_idle": (_i, [_vp, _u32, _u32]),
     "vfr_server_destroy": (None, [_vp]),
     "vfr_find_visible_static": (_i, [_vp, _u32, _vp, _u32, _vp, _u32, _vp, _vp, _vp]),
     "vfr_psi_table": (_i, [_vp]),

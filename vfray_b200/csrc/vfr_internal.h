@@ -12,15 +12,21 @@
 
 namespace vfr {
 
-// Grow-only device buffer.
+// Grow-only device buffer, or a piece of an Arena (owned = false: never
+// freed by the buffer).
 struct Buf {
   void* p = nullptr;
   size_t cap = 0;
+  bool owned = true;
   Buf() = default;
   Buf(const Buf&) = delete;
   Buf& operator=(const Buf&) = delete;
-  ~Buf() {
-    if (p) cudaFree(p);
+  ~Buf() { release(); }
+  void release() {
+    if (p && owned) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    owned = true;
   }
   template <class T>
   T* as(size_t byte_off = 0) const {
@@ -60,6 +66,13 @@ struct Tuning {
 
 struct Ctx;
 
+// A region of device memory that batches are laid out in by bumping an
+// offset (the served form's arena): nothing is allocated or freed per batch.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, off = 0;
+};
+
 // One render job as the caller describes it.
 struct JobSpec {
   int mesh = -1;
@@ -79,21 +92,28 @@ struct Batch {
   std::vector<JobSpec> specs;
   std::vector<JobDev> jobs;
   uint32_t njobs = 0;
-  // host-known prefixes: view blocks, edge blocks, ext-face blocks, tiles
-  std::vector<uint32_t> pref;  // 4 arrays of njobs + 1
-  uint32_t rot_blocks = 0, edge_blocks = 0, ext_blocks = 0, tiles = 0;
+  // host-known prefixes: view blocks, edge blocks, ext-face blocks, ray-list
+  // tiles, screen tiles (composited stage (b))
+  std::vector<uint32_t> pref;  // 5 arrays of njobs + 1
+  uint32_t rot_blocks = 0, edge_blocks = 0, ext_blocks = 0, tiles = 0, stiles = 0;
   size_t pixels = 0, ext_total = 0;
   uint64_t scratch_bytes = 0;
   Buf d_jobs, d_pref, d_dev_pref, d_ctr;  // d_dev_pref: vis prefix, ray prefix, queue
-  Buf vview, planes, blk, vis, bbox, winner, rays, ent_cnt, ent_off, ent_cur, ent, scan;
+  Buf vview, planes, blk, vis, bbox, winner, rays, ent_cnt, ent_off, ent, scan;
+  Buf tile_cnt, tile_off, tile_cur, bins;  // composited: faces binned by screen tile
   Buf out_rgb8, out_rgba, out_steps;      // outputs owned by the batch (host-output calls)
-  size_t ent_cap = 0;
+  size_t ent_cap = 0, bin_cap = 0;  // composited: entry and bin capacities (0: sized at layout)
   cudaGraphExec_t exec = nullptr;
   cudaStream_t stream = nullptr;  // null: the context's stream
   cudaStream_t st() const;
   // pinned staging for the per-call upload of a one-job batch
   void* stage = nullptr;
   size_t stage_cap = 0;
+  // or the caller's pinned staging (not owned; the served form's pool): a
+  // pinned allocation waits for all work on the device, a running served
+  // launch included
+  char* ext_stage = nullptr;
+  size_t ext_stage_cap = 0;
   cudaEvent_t stage_done = nullptr;
 
   ~Batch();
@@ -101,7 +121,18 @@ struct Batch {
   uint32_t* ray_pref() const { return d_dev_pref.as<uint32_t>((njobs + 1) * 4); }
   uint32_t* queue() const { return d_dev_pref.as<uint32_t>(2 * (njobs + 1) * 4); }
   uint32_t tile_w = 8;  // the tile shape the layout was made for
+  // Where the buffers come from: grow-only allocations of the batch's own,
+  // or (arena set) consecutive pieces of the arena from its offset on.
+  Arena* arena = nullptr;
+  bool rgb8_only = false;  // owned outputs: RGB8 only (no float RGBA, no steps)
+  // Threads of the stage (a) and scan blocks: 1024, or 256 so that the
+  // chain fits beside the served launch (CTAs of at most 256 threads).
+  uint32_t fb = 1024;
   int layout(const std::vector<JobSpec>& s, int mode, bool own_outputs);
+  int place(Buf& b, size_t bytes, const char* what);
+  // Arena bytes a layout of these jobs takes (an upper bound).
+  static size_t arena_bytes(Ctx& C, const std::vector<JobSpec>& s, int mode, uint32_t fb,
+                            bool rgb8_only);
   int upload(bool async);
   int enqueue_a();
   int enqueue_b();
@@ -115,6 +146,7 @@ struct Batch {
   int capture();
   int run();
   int counters(std::vector<ViewCounters>& out);
+  bool overflowed(const std::vector<ViewCounters>& k);
   void drop_graph();
 };
 
@@ -131,7 +163,7 @@ struct Ctx {
   cudaEvent_t ev[4] = {};
   int occ[4] = {0, 0, 0, 0};
   uint32_t step_cap = 0;
-  size_t ent_cap_hint = 0;
+  size_t ent_cap_hint = 0, bin_cap_hint = 0;
   Tuning tune;
   bool profile = false;
   struct StageEvents {
@@ -151,6 +183,14 @@ struct Ctx {
   const void* traverse_fn(int mode, uint32_t variant);
   int check_status(uint32_t status, uint32_t nentries_over);
 };
+
+// The served form's launches (vfr_render.cu, where the kernels are
+// compiled): the drain, its occupancy, and the publication of a segment.
+int serve_blocks_per_sm(int* n);
+cudaError_t launch_serve(const ServeParams& sp, int grid, cudaStream_t st);
+cudaError_t launch_publish(SegDev* segs, ServeCtl* ctl, uint32_t seq, const JobDev* jobs,
+                           const uint32_t* ray_pref, uint32_t* done, uint32_t njobs,
+                           cudaStream_t st);
 
 }  // namespace vfr
 

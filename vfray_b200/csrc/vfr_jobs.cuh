@@ -30,11 +30,14 @@ __device__ __forceinline__ float job_maxedge(const JobDev& J) {
 __global__ void init_jobs_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
                                  uint32_t* __restrict__ queue) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j == 0) *queue = 0;
+  if (j == 0) {
+    queue[0] = 0;  // the traversal's ray queue
+    queue[1] = 0;  // the composited mode's entry-arena cursor
+  }
   if (j >= njobs) return;
   ViewCounters v;
   v.nvis = 0; v.nrays = 0; v.nentries = 0; v.status = 0; v.steps = 0;
-  v.maxedge_bits = 0; v.rays_done = 0;
+  v.maxedge_bits = 0; v.rays_done = 0; v.nbins = 0;
   for (int k = 0; k < 4; ++k) { v.mm[k] = 0xffffffffu; v.mm[4 + k] = 0u; }
   *jobs[j].ctr = v;
 }
@@ -234,12 +237,13 @@ __global__ void __launch_bounds__(1024) compact_kernel(const JobDev* __restrict_
   const uint32_t nb = bpref[j + 1] - bpref[j];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t part = 0;
+  const uint32_t nwarps = blockDim.x >> 5;  // blocks of 256 or 1024 threads
   for (uint32_t b = threadIdx.x; b < lb; b += blockDim.x) part += J.blk[b];
   for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
   if (lane == 0) s_warp[warp] = part;
   __syncthreads();
   if (warp == 0) {
-    uint32_t x = s_warp[lane];
+    uint32_t x = lane < nwarps ? s_warp[lane] : 0u;
     for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     if (lane == 0) s_base = x;
   }
@@ -250,7 +254,7 @@ __global__ void __launch_bounds__(1024) compact_kernel(const JobDev* __restrict_
   if (lane == 0) s_warp[warp] = __popc(m);
   __syncthreads();
   if (warp == 0) {
-    const uint32_t c = s_warp[lane];
+    const uint32_t c = lane < nwarps ? s_warp[lane] : 0u;
     uint32_t x = c;
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -287,7 +291,7 @@ __global__ void __launch_bounds__(1024) prefix_kernel(const JobDev* __restrict__
     if (lane == 31) s[warp] = x;
     __syncthreads();
     if (warp == 0) {
-      const uint32_t c = s[lane];
+      const uint32_t c = lane < (blockDim.x >> 5) ? s[lane] : 0u;
       uint32_t z = c;
       for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
@@ -307,6 +311,24 @@ __global__ void __launch_bounds__(1024) prefix_kernel(const JobDev* __restrict__
 
 // ------------------------------------------------------------ stage (b)
 
+// projectVisibleFaces (vfRayKernelCPU.cc:136-169): the pixel bounding box of
+// a face from its vertex xy, which stage (a) stores with the plane (p1.zw,
+// p2.xy, p2.zw); min starts at res - 1 and max at 0 as in the reference.
+__device__ __forceinline__ uint4 face_box(const float4& p1, const float4& p2, uint32_t W,
+                                          uint32_t H) {
+  uint32_t bx = W - 1, by = H - 1, bz = 0, bw = 0;
+  const float xs[3] = {p1.z, p2.x, p2.z}, ys[3] = {p1.w, p2.y, p2.w};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t ix = to_pixel(xs[k], W), iy = to_pixel(ys[k], H);
+    if (ix < bx) bx = ix;
+    if (iy < by) by = iy;
+    if (ix > bz) bz = ix;
+    if (iy > bw) bw = iy;
+  }
+  return make_uint4(bx, by, bz, bw);
+}
+
 // projectVisibleFaces (vfRayKernelCPU.cc:136-169) + the pixel coverage of
 // vfRay's face loop (:248-274): persistent warps over the visible faces of
 // all jobs, one warp per face, its lanes over the pixels of the face's
@@ -319,12 +341,10 @@ __global__ void __launch_bounds__(1024) prefix_kernel(const JobDev* __restrict__
 // face in order write a pixel; visible order is ext-face order, so the
 // winner is the largest ext-face index reaching it: atomicMax.  Pixels
 // outside the image are clipped (the reference would write past its buffer
-// there).  kCount/kFill: the composited mode's entry-list passes, which
-// skip only the pixel itself.
-template <bool kCount, bool kFill>
+// there).  Reference mode; the composited mode's entry lists come from the
+// screen-tile kernels below.
 __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
-                                                     const uint32_t* __restrict__ vpref,
-                                                     uint2* __restrict__ ent, uint32_t ent_cap) {
+                                                     const uint32_t* __restrict__ vpref) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t total = vpref[njobs];
@@ -341,17 +361,9 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
     const float4 v0 = make_float4(p1.z, p1.w, 0.0f, 0.0f);
     const float4 v1 = make_float4(p2.x, p2.y, 0.0f, 0.0f);
     const float4 v2 = make_float4(p2.z, p2.w, 0.0f, 0.0f);
-    uint32_t bx = W - 1, by = H - 1, bz = 0, bw = 0;
-    const float4 vv[3] = {v0, v1, v2};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const uint32_t ix = to_pixel(vv[k].x, W), iy = to_pixel(vv[k].y, H);
-      if (ix < bx) bx = ix;
-      if (iy < by) by = iy;
-      if (ix > bz) bz = ix;
-      if (iy > bw) bw = iy;
-    }
-    if (!kFill && lane == 0) J.bbox[i] = make_uint4(bx, by, bz, bw);
+    const uint4 box = face_box(p1, p2, W, H);
+    const uint32_t bx = box.x, by = box.y, bz = box.z, bw = box.w;
+    if (lane == 0) J.bbox[i] = box;
     const uint32_t xe = min(bz, W - 1), ye = min(bw, H - 1);
     if (bx > xe || by > ye) continue;  // box entirely outside the image
     const EntryEdges E = entry_edges(v0, v1, v2);
@@ -378,22 +390,202 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
           ok = (sp >= 0.0f) && (sp <= 1.0f);
         }
         const uint32_t p = py * W + px;
-        if (kCount || kFill) {
-          if (live && inside && ok) {
-            if (kCount) {
-              atomicAdd(&J.ent_cnt[p], 1u);
-            } else {
-              const float zp = plane_eval(ox, oy, p0.x, p0.y, p0.z);
-              const uint32_t slot = J.ent_off[p] + atomicAdd(&J.ent_cur[p], 1u);
-              if (slot < ent_cap) ent[slot] = make_uint2(__float_as_uint(zp), e);
-            }
-          }
-        } else {
-          const uint32_t kill = __ballot_sync(0xffffffffu, live && inside && !ok);
-          if (live && inside && ok && !carried && !(kill & upto)) atomicMax(&J.winner[p], (int32_t)e);
-          carried = carried || (kill & seg);
-        }
+        const uint32_t kill = __ballot_sync(0xffffffffu, live && inside && !ok);
+        if (live && inside && ok && !carried && !(kill & upto)) atomicMax(&J.winner[p], (int32_t)e);
+        carried = carried || (kill & seg);
       }
+    }
+  }
+}
+
+// ------------------------------------------------------------ stage (b), composited mode
+//
+// Every visible face covering a pixel (entry scalar in [0, 1]) is an entry
+// of that pixel's ray.  The faces are binned into screen tiles of 16 x 16
+// pixels (count, scan, fill: one atomic per face and tile), then one CTA per
+// tile stages the tile's faces in shared memory, and each thread tests its
+// pixel against them and writes its pixel's entry list in descending
+// (depth, face) order -- the order the traversal takes the segments in.
+
+constexpr uint32_t kTile = 16;
+
+// Bin pass over the visible faces of all jobs: kFill = false counts the
+// screen tiles each face's box overlaps (and stores the box), kFill = true
+// writes the face's visible index into each tile's bin.  tpref: prefix of
+// the jobs' tile counts.
+template <bool kFill>
+__global__ void __launch_bounds__(256) bin_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
+                                                  const uint32_t* __restrict__ vpref,
+                                                  const uint32_t* __restrict__ tpref,
+                                                  uint32_t* __restrict__ tile_cnt,
+                                                  const uint32_t* __restrict__ tile_off,
+                                                  uint32_t* __restrict__ tile_cur,
+                                                  uint32_t* __restrict__ bins, uint32_t bin_cap) {
+  const uint32_t total = vpref[njobs];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t g0 = blockIdx.x * blockDim.x; g0 < total; g0 += stride) {
+    const uint32_t g = g0 + threadIdx.x;
+    uint32_t j = 0, n = 0;
+    if (g < total) {
+      j = job_of(vpref, njobs, g);
+      const JobDev& J = jobs[j];
+      const uint32_t i = g - vpref[j];
+      const float4* pl = J.planes + kPlaneStride * (size_t)J.vis_ext[i];
+      const uint4 b = face_box(pl[1], pl[2], J.W, J.H);
+      if (!kFill) J.bbox[i] = b;
+      const uint32_t xe = min(b.z, J.W - 1), ye = min(b.w, J.H - 1);
+      if (b.x <= xe && b.y <= ye) {
+        const uint32_t tpx = (J.W + kTile - 1) / kTile, base = tpref[j];
+        for (uint32_t ty = b.y / kTile; ty <= ye / kTile; ++ty)
+          for (uint32_t tx = b.x / kTile; tx <= xe / kTile; ++tx) {
+            const uint32_t t = base + ty * tpx + tx;
+            if (!kFill) {
+              atomicAdd(&tile_cnt[t], 1u);
+            } else {
+              const uint32_t slot = tile_off[t] + atomicAdd(&tile_cur[t], 1u);
+              if (slot < bin_cap) bins[slot] = i;
+            }
+            ++n;
+          }
+      }
+    }
+    if (!kFill) {  // per job the (face, tile) pairs, one atomic per job and warp
+      const uint32_t act = __activemask();
+      const uint32_t peers = __match_any_sync(act, g < total ? j : 0xffffffffu);
+      const uint32_t sum = __reduce_add_sync(peers, n);
+      if (g < total && (threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1) && sum)
+        atomicAdd(&jobs[j].ctr->nbins, sum);
+    }
+  }
+}
+
+// A face as the tile kernel tests it: its box, entry edges, depth and
+// scalar planes, ext-face index.
+struct TileFace {
+  uint4 box;
+  EntryEdges E;
+  float zx, zy, zz, sx, sy, sz;
+  uint32_t e;
+};
+
+// One CTA per screen tile (a block-stride loop over the tiles of all jobs),
+// one thread per pixel.  Pass 1 counts each pixel's entries; a block scan
+// and one atomic on the batch's entry cursor give each pixel its list's
+// place; pass 2 inserts each entry into its pixel's list in descending
+// (depth, face) order.  The entry test is the rasteriser's own: the pixel in
+// the face's box (clipped to the image), inside the entry face (inclusive,
+// vfRayKernelCPU.cc:258-268), entry scalar in [0, 1].  Lists that do not
+// fit the arena are left empty and counted, and the caller renders again
+// with room (as with bins past their capacity).
+__global__ void __launch_bounds__(256) tile_kernel(const JobDev* __restrict__ jobs, uint32_t njobs,
+                                                   const uint32_t* __restrict__ tpref,
+                                                   const uint32_t* __restrict__ tile_off,
+                                                   const uint32_t* __restrict__ bins,
+                                                   uint32_t bin_cap, uint2* __restrict__ ent,
+                                                   uint32_t ent_cap, uint32_t* __restrict__ cursor) {
+  __shared__ TileFace F[256];
+  __shared__ uint32_t s_warp[8];
+  __shared__ uint32_t s_base;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t ntiles = tpref[njobs];
+  for (uint32_t g = blockIdx.x; g < ntiles; g += gridDim.x) {
+    const uint32_t j = job_of(tpref, njobs, g);
+    const JobDev& J = jobs[j];
+    const uint32_t lt = g - tpref[j], W = J.W, H = J.H;
+    const uint32_t tpx = (W + kTile - 1) / kTile;
+    const uint32_t px = (lt % tpx) * kTile + (tid % kTile), py = (lt / tpx) * kTile + tid / kTile;
+    const bool live = px < W && py < H;
+    const double rW = __drcp_rn((double)(float)(W - 1u)), rH = __drcp_rn((double)(float)(H - 1u));
+    const float ox = obj_coord_r(px, rW), oy = obj_coord_r(py, rH);
+    const uint32_t b0 = min(tile_off[g], bin_cap), b1 = min(tile_off[g + 1], bin_cap);
+    auto covers = [&](const TileFace& f) {
+      return px >= f.box.x && px <= min(f.box.z, W - 1) && py >= f.box.y &&
+             py <= min(f.box.w, H - 1) && entry_inside(f.E, ox, oy) && [&] {
+               const float sp = plane_eval(ox, oy, f.sx, f.sy, f.sz);
+               return (sp >= 0.0f) && (sp <= 1.0f);
+             }();
+    };
+    auto stage = [&](uint32_t c) {  // faces c .. c+255 of the bin into shared memory
+      __syncthreads();
+      if (c + tid < b1) {
+        const uint32_t i = bins[c + tid];
+        const uint32_t e = J.vis_ext[i];
+        const float4* pl = J.planes + kPlaneStride * (size_t)e;
+        const float4 p0 = pl[0], p1 = pl[1], p2 = pl[2];
+        TileFace f;
+        f.box = J.bbox[i];
+        f.E = entry_edges(make_float4(p1.z, p1.w, 0.0f, 0.0f), make_float4(p2.x, p2.y, 0.0f, 0.0f),
+                          make_float4(p2.z, p2.w, 0.0f, 0.0f));
+        f.zx = p0.x;
+        f.zy = p0.y;
+        f.zz = p0.z;
+        f.sx = p0.w;
+        f.sy = p1.x;
+        f.sz = p1.y;
+        f.e = e;
+        F[tid] = f;
+      }
+      __syncthreads();
+      return min(256u, b1 - c);
+    };
+    // pass 1: entries per pixel
+    uint32_t count = 0;
+    for (uint32_t c = b0; c < b1; c += 256) {
+      const uint32_t m = stage(c);
+      if (live)
+        for (uint32_t k = 0; k < m; ++k) count += covers(F[k]) ? 1u : 0u;
+    }
+    // block scan of the counts
+    uint32_t x = count;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t c = lane < 8 ? s_warp[lane] : 0u;
+      uint32_t z = c;
+      for (int o = 1; o < 8; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= (uint32_t)o) z += y;
+      }
+      if (lane < 8) s_warp[lane] = z - c;
+      if (lane == 7) {
+        s_base = atomicAdd(cursor, z);
+        atomicAdd(&J.ctr->nentries, z);
+      }
+    }
+    __syncthreads();
+    const uint32_t off = s_base + s_warp[warp] + x - count;
+    const bool fits = off + count <= ent_cap;
+    // VFR_DEV_OVERFLOW: a list or this tile's bin did not fit
+    if ((live && count && !fits) || (tid == 0 && tile_off[g + 1] > bin_cap))
+      atomicOr(&J.ctr->status, 16u);
+    if (live) {
+      const uint32_t p = py * W + px;
+      J.ent_off[p] = fits ? off : 0u;
+      J.ent_cnt[p] = fits ? count : 0u;
+    }
+    // pass 2: each pixel's entries, inserted in descending (depth, face) order
+    uint32_t n = 0;
+    for (uint32_t c = b0; c < b1; c += 256) {
+      const uint32_t m = stage(c);
+      if (live && fits && count)
+        for (uint32_t k = 0; k < m; ++k) {
+          const TileFace& f = F[k];
+          if (!covers(f)) continue;
+          const float z = plane_eval(ox, oy, f.zx, f.zy, f.zz);
+          uint32_t q = n++;
+          while (q > 0) {
+            const uint2 a = ent[off + q - 1];
+            const float za = __uint_as_float(a.x);
+            if (za > z || (za == z && a.y > f.e)) break;
+            ent[off + q] = a;
+            --q;
+          }
+          ent[off + q] = make_uint2(__float_as_uint(z), f.e);
+        }
     }
   }
 }
@@ -456,7 +648,7 @@ __global__ void __launch_bounds__(1024) scan_blocks_kernel(const uint32_t* __res
   if (lane == 31) s[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    const uint32_t c = s[lane];
+    const uint32_t c = lane < (blockDim.x >> 5) ? s[lane] : 0u;
     uint32_t z = c;
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
@@ -481,7 +673,7 @@ __global__ void __launch_bounds__(1024) scan_add_kernel(uint32_t* __restrict__ o
   if (lane == 0) s[warp] = part;
   __syncthreads();
   if (warp == 0) {
-    uint32_t x = s[lane];
+    uint32_t x = lane < (blockDim.x >> 5) ? s[lane] : 0u;
     for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     if (lane == 0) s_base = x;
   }
@@ -489,15 +681,6 @@ __global__ void __launch_bounds__(1024) scan_add_kernel(uint32_t* __restrict__ o
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] += s_base;
   if (total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *total = s_base + sums[blockIdx.x];
-}
-
-// Per-job entry totals for the composited mode (for stats and overflow).
-__global__ void entry_totals_kernel(const JobDev* __restrict__ jobs, uint32_t njobs) {
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= njobs) return;
-  const JobDev& J = jobs[j];
-  const uint32_t np = J.W * J.H;
-  J.ctr->nentries = J.ent_off[np] - J.ent_off[0];
 }
 
 }  // namespace vfr

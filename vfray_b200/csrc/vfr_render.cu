@@ -128,7 +128,7 @@ int Ctx::traverse_blocks_per_sm(int mode) {
 }
 
 int Ctx::check_status(uint32_t status, uint32_t overflow) {
-  if (overflow) return fail(VFR_ERR_DEVICE, "entry lists overflowed; render again");
+  if (overflow) return fail(VFR_ERR_DEVICE, "entry lists or tile bins overflowed; render again");
   if (status & (VFR_DEV_CYCLE | VFR_DEV_RANGE | VFR_DEV_STEP_CAP | VFR_DEV_OVERFLOW)) {
     char buf[128];
     std::snprintf(buf, sizeof buf, "device status 0x%x (step-cap=2 range=4 overflow=16 cycle=32)",
@@ -204,6 +204,51 @@ int Ctx::mesh_edges(Mesh* m, cudaStream_t st) {
 
 // Lays the jobs out in the batch's arenas (allocating what is missing) and
 // fills the job table on the host.
+// A buffer of the layout: grown (the batch's own memory) or the next piece
+// of the arena, 256-byte aligned.
+int Batch::place(Buf& b, size_t bytes, const char* what) {
+  if (!arena) return ctx->grow(b, bytes, what);
+  const size_t need = (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
+  if (arena->off + need > arena->cap) return ctx->fail(VFR_ERR_BUDGET, std::string(what) + ": arena full");
+  b.release();
+  b.p = arena->base + arena->off;
+  b.cap = need;
+  b.owned = false;
+  arena->off += need;
+  return VFR_OK;
+}
+
+// The arena bytes layout() places for these jobs: every buffer kind's total
+// rounded up to 256 bytes (the same sizes, in the same order).
+size_t Batch::arena_bytes(Ctx& C, const std::vector<JobSpec>& s, int mode, uint32_t fb,
+                          bool rgb8_only) {
+  const size_t nj = s.size();
+  size_t nv_mv = 0, next = 0, nblk = 0, pix = 0, stiles = 0;
+  for (const JobSpec& q : s) {
+    const Mesh* m = C.mesh(q.mesh);
+    if (!m) continue;
+    nv_mv += q.use_mv ? m->nV : 0;
+    next += m->nExt;
+    nblk += cdiv(m->nExt, fb);
+    pix += (size_t)q.W * q.H;
+    stiles += (size_t)cdiv(q.W, kTile) * cdiv(q.H, kTile);
+  }
+  auto a = [](size_t b) { return (std::max<size_t>(b, 16) + 255) & ~(size_t)255; };
+  size_t t = a(sizeof(JobDev) * nj) + a(sizeof(uint32_t) * 5 * (nj + 1)) +
+             a(sizeof(uint32_t) * (2 * (nj + 1) + 4)) + a(sizeof(ViewCounters) * nj) +
+             a(sizeof(float4) * nv_mv) + a(sizeof(float4) * kPlaneStride * next) +
+             a(sizeof(uint32_t) * nblk) + a(sizeof(uint32_t) * next) + a(sizeof(uint4) * next) +
+             a(sizeof(uint32_t) * pix);
+  if (mode == VFR_MODE_REF) t += a(sizeof(int32_t) * pix);
+  if (mode == VFR_MODE_COMPOSITED)
+    t += 2 * a(sizeof(uint32_t) * pix) + 2 * a(sizeof(uint32_t) * (stiles + 1)) +
+         a(sizeof(uint32_t) * stiles) + a(sizeof(uint32_t) * (cdiv(stiles + 1, fb) + 1)) +
+         a(sizeof(uint32_t) * (32 * stiles + 4 * next)) + a(sizeof(uint2) * (pix * 4 + 1024));
+  t += a(3 * pix);
+  if (!rgb8_only) t += a(sizeof(float4) * pix) + a(sizeof(uint32_t) * pix);
+  return t;
+}
+
 int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
   Ctx& C = *ctx;
   specs = s;
@@ -211,11 +256,12 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
   tile_w = C.tune.tile_w;
   njobs = (uint32_t)s.size();
   jobs.assign(njobs, JobDev{});
-  pref.assign(4 * (size_t)(njobs + 1), 0);
+  pref.assign(5 * (size_t)(njobs + 1), 0);
   uint32_t* pr = pref.data();
   uint32_t* pe = pr + (njobs + 1);
   uint32_t* px = pe + (njobs + 1);
   uint32_t* pt = px + (njobs + 1);
+  uint32_t* ps = pt + (njobs + 1);  // composited: 16 x 16 screen tiles
   size_t nv_mv = 0, next = 0, nblk = 0, pix = 0;
   for (uint32_t j = 0; j < njobs; ++j) {
     Mesh* mesh = C.mesh(s[j].mesh);
@@ -225,19 +271,23 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
       return C.fail(VFR_ERR_INVALID, "image size out of range");
     const uint32_t rb =
         q.use_mv ? std::max<uint32_t>(1, std::min<uint32_t>(cdiv(mesh->nV, 1024), 2 * C.num_sms)) : 0;
-    if (q.use_mv) {
+    if (q.use_mv && !mesh->edges) {
+      // built once per mesh (allocates and waits): a server builds them all
+      // before its launch starts
+      if (arena) return C.fail(VFR_ERR_STATE, "mesh edges missing for an arena layout");
       const int rc = C.mesh_edges(mesh, st());
       if (rc) return rc;
     }
     const uint32_t eb =
         q.use_mv ? std::max<uint32_t>(1, std::min<uint32_t>(cdiv(mesh->nEdges, 1024), 4 * C.num_sms))
                  : 0;
-    const uint32_t xb = cdiv(mesh->nExt, 1024);
+    const uint32_t xb = cdiv(mesh->nExt, fb);
     const uint32_t tl = cdiv(q.W, C.tune.tile_w) * cdiv(q.H, 32 / C.tune.tile_w);
     pr[j + 1] = pr[j] + rb;
     pe[j + 1] = pe[j] + eb;
     px[j + 1] = px[j] + xb;
     pt[j + 1] = pt[j] + tl;
+    ps[j + 1] = ps[j] + cdiv(q.W, kTile) * cdiv(q.H, kTile);
     nv_mv += q.use_mv ? mesh->nV : 0;
     next += mesh->nExt;
     nblk += xb;
@@ -247,41 +297,48 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
   edge_blocks = pe[njobs];
   ext_blocks = px[njobs];
   tiles = pt[njobs];
+  stiles = ps[njobs];
   pixels = pix;
   ext_total = next;
   if (pix > 0xffffffffull || next > 0xffffffffull) return C.fail(VFR_ERR_BUDGET, "batch too large");
   const size_t old_sig = (size_t)vview.p ^ (size_t)planes.p ^ (size_t)winner.p ^ (size_t)rays.p ^
                          (size_t)ent.p ^ (size_t)d_jobs.p;
-  int rc = C.grow(d_jobs, sizeof(JobDev) * njobs, "job table");
-  if (!rc) rc = C.grow(d_pref, sizeof(uint32_t) * pref.size(), "job prefixes");
-  if (!rc) rc = C.grow(d_dev_pref, sizeof(uint32_t) * (2 * (size_t)(njobs + 1) + 4), "device prefixes");
-  if (!rc) rc = C.grow(d_ctr, sizeof(ViewCounters) * njobs, "view counters");
-  if (!rc) rc = C.grow(vview, sizeof(float4) * nv_mv, "view vertices");
-  if (!rc) rc = C.grow(planes, sizeof(float4) * kPlaneStride * next, "planes");
-  if (!rc) rc = C.grow(blk, sizeof(uint32_t) * nblk, "block counts");
-  if (!rc) rc = C.grow(vis, sizeof(uint32_t) * next, "visible lists");
-  if (!rc) rc = C.grow(bbox, sizeof(uint4) * next, "bboxes");
-  if (!rc) rc = C.grow(rays, sizeof(uint32_t) * pix, "ray lists");
-  if (!rc && mode == VFR_MODE_REF) rc = C.grow(winner, sizeof(int32_t) * pix, "winner maps");
+  int rc = place(d_jobs, sizeof(JobDev) * njobs, "job table");
+  if (!rc) rc = place(d_pref, sizeof(uint32_t) * pref.size(), "job prefixes");
+  if (!rc) rc = place(d_dev_pref, sizeof(uint32_t) * (2 * (size_t)(njobs + 1) + 4), "device prefixes");
+  if (!rc) rc = place(d_ctr, sizeof(ViewCounters) * njobs, "view counters");
+  if (!rc) rc = place(vview, sizeof(float4) * nv_mv, "view vertices");
+  if (!rc) rc = place(planes, sizeof(float4) * kPlaneStride * next, "planes");
+  if (!rc) rc = place(blk, sizeof(uint32_t) * nblk, "block counts");
+  if (!rc) rc = place(vis, sizeof(uint32_t) * next, "visible lists");
+  if (!rc) rc = place(bbox, sizeof(uint4) * next, "bboxes");
+  if (!rc) rc = place(rays, sizeof(uint32_t) * pix, "ray lists");
+  if (!rc && mode == VFR_MODE_REF) rc = place(winner, sizeof(int32_t) * pix, "winner maps");
   if (!rc && mode == VFR_MODE_COMPOSITED) {
-    if (ent_cap == 0) ent_cap = C.ent_cap_hint ? C.ent_cap_hint : pix * 4 + 1024;
-    rc = C.grow(ent_cnt, sizeof(uint32_t) * (pix + 1), "entry counts");
-    if (!rc) rc = C.grow(ent_off, sizeof(uint32_t) * (pix + 1), "entry offsets");
-    if (!rc) rc = C.grow(ent_cur, sizeof(uint32_t) * pix, "entry cursors");
-    if (!rc) rc = C.grow(scan, sizeof(uint32_t) * (cdiv(pix + 1, 1024) + 1), "scan sums");
-    if (!rc) rc = C.grow(ent, sizeof(uint2) * ent_cap, "entries");
+    if (ent_cap == 0) ent_cap = (C.ent_cap_hint && !arena) ? C.ent_cap_hint : pix * 4 + 1024;
+    if (bin_cap == 0)
+      bin_cap = (C.bin_cap_hint && !arena) ? C.bin_cap_hint : 32 * (size_t)stiles + 4 * next;
+    rc = place(ent_cnt, sizeof(uint32_t) * pix, "entry counts");
+    if (!rc) rc = place(ent_off, sizeof(uint32_t) * pix, "entry offsets");
+    if (!rc) rc = place(tile_cnt, sizeof(uint32_t) * (stiles + 1), "tile counts");
+    if (!rc) rc = place(tile_off, sizeof(uint32_t) * (stiles + 1), "tile offsets");
+    if (!rc) rc = place(tile_cur, sizeof(uint32_t) * stiles, "tile cursors");
+    if (!rc) rc = place(scan, sizeof(uint32_t) * (cdiv(stiles + 1, fb) + 1), "scan sums");
+    if (!rc) rc = place(bins, sizeof(uint32_t) * bin_cap, "tile bins");
+    if (!rc) rc = place(ent, sizeof(uint2) * ent_cap, "entries");
   }
   if (!rc && own_outputs) {
-    rc = C.grow(out_rgb8, 3 * pix, "rgb8 outputs");
-    if (!rc) rc = C.grow(out_rgba, sizeof(float4) * pix, "rgba outputs");
-    if (!rc) rc = C.grow(out_steps, sizeof(uint32_t) * pix, "steps outputs");
+    rc = place(out_rgb8, 3 * pix, "rgb8 outputs");
+    if (!rc && !rgb8_only) rc = place(out_rgba, sizeof(float4) * pix, "rgba outputs");
+    if (!rc && !rgb8_only) rc = place(out_steps, sizeof(uint32_t) * pix, "steps outputs");
   }
   if (rc) return rc;
   const size_t new_sig = (size_t)vview.p ^ (size_t)planes.p ^ (size_t)winner.p ^ (size_t)rays.p ^
                          (size_t)ent.p ^ (size_t)d_jobs.p;
   if (new_sig != old_sig) drop_graph();
   scratch_bytes = vview.cap + planes.cap + blk.cap + vis.cap + bbox.cap + rays.cap + winner.cap +
-                  ent_cnt.cap + ent_off.cap + ent_cur.cap + ent.cap + scan.cap + d_ctr.cap;
+                  ent_cnt.cap + ent_off.cap + tile_cnt.cap + tile_off.cap + tile_cur.cap + bins.cap +
+                  ent.cap + scan.cap + d_ctr.cap;
   size_t ov = 0, oe = 0, ob = 0, op = 0;
   for (uint32_t j = 0; j < njobs; ++j) {
     Mesh* mesh = C.mesh(s[j].mesh);
@@ -306,15 +363,14 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     J.rays = rays.as<uint32_t>(sizeof(uint32_t) * op);
     J.ent_cnt = mode == VFR_MODE_COMPOSITED ? ent_cnt.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
     J.ent_off = mode == VFR_MODE_COMPOSITED ? ent_off.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
-    J.ent_cur = mode == VFR_MODE_COMPOSITED ? ent_cur.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
     J.ctr = d_ctr.as<ViewCounters>(sizeof(ViewCounters) * j);
     J.ent = mode == VFR_MODE_COMPOSITED ? ent.as<uint2>() : nullptr;
     J.ent_cap = (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu);
     J.mode = (uint32_t)mode;
     if (own_outputs) {
       specs[j].rgb8 = out_rgb8.as<uint8_t>(3 * op);
-      specs[j].rgba = out_rgba.as<float4>(sizeof(float4) * op);
-      specs[j].steps = out_steps.as<uint32_t>(sizeof(uint32_t) * op);
+      specs[j].rgba = rgb8_only ? nullptr : out_rgba.as<float4>(sizeof(float4) * op);
+      specs[j].steps = rgb8_only ? nullptr : out_steps.as<uint32_t>(sizeof(uint32_t) * op);
     }
     J.rgb8 = specs[j].rgb8;
     J.rgba = specs[j].rgba;
@@ -329,7 +385,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     J.pix_base = (uint32_t)op;
     ov += q.use_mv ? mesh->nV : 0;
     oe += mesh->nExt;
-    ob += cdiv(mesh->nExt, 1024);
+    ob += cdiv(mesh->nExt, fb);
     op += (size_t)q.W * q.H;
   }
   return VFR_OK;
@@ -347,6 +403,17 @@ int Batch::upload(bool async) {
       rc = C.cuda(cudaMemcpyAsync(d_pref.p, pref.data(), bp, cudaMemcpyHostToDevice, st()),
                   "prefix upload");
     if (!rc) rc = C.cuda(cudaStreamSynchronize(st()), "upload");
+    return rc;
+  }
+  if (ext_stage) {  // the caller's pinned staging, used once (no allocation, no wait)
+    if (ext_stage_cap < bj + bp) return C.fail(VFR_ERR_INVALID, "staging too small");
+    std::memcpy(ext_stage, jobs.data(), bj);
+    std::memcpy(ext_stage + bj, pref.data(), bp);
+    int rc = C.cuda(cudaMemcpyAsync(d_jobs.p, ext_stage, bj, cudaMemcpyHostToDevice, st()),
+                    "job table upload");
+    if (!rc)
+      rc = C.cuda(cudaMemcpyAsync(d_pref.p, ext_stage + bj, bp, cudaMemcpyHostToDevice, st()),
+                  "prefix upload");
     return rc;
   }
   if (!stage_done) cudaEventCreateWithFlags(&stage_done, cudaEventDisableTiming);
@@ -383,10 +450,10 @@ int Batch::enqueue_a() {
     view_maxedge_kernel<<<edge_blocks, 256, 0, st>>>(J, njobs, P + n1);
   }
   if (ext_blocks) {
-    visible_kernel<<<ext_blocks, 1024, 0, st>>>(J, njobs, P + 2 * n1);
-    compact_kernel<<<ext_blocks, 1024, 0, st>>>(J, njobs, P + 2 * n1);
+    visible_kernel<<<ext_blocks, fb, 0, st>>>(J, njobs, P + 2 * n1);
+    compact_kernel<<<ext_blocks, fb, 0, st>>>(J, njobs, P + 2 * n1);
   }
-  prefix_kernel<<<1, 1024, 0, st>>>(J, njobs, 0, vis_pref());
+  prefix_kernel<<<1, fb, 0, st>>>(J, njobs, 0, vis_pref());
   return C.cuda(cudaGetLastError(), "stage (a) launch");
 }
 
@@ -399,21 +466,29 @@ int Batch::enqueue_b() {
   const uint32_t rb = std::max(1, C.num_sms * (int)C.tune.raster_warps_per_sm / 8);
   if (mode == VFR_MODE_REF) {
     cudaMemsetAsync(winner.p, 0xff, sizeof(int32_t) * pixels, st);
-    raster_kernel<false, false><<<rb, 256, 0, st>>>(J, njobs, vis_pref(), nullptr, 0);
+    raster_kernel<<<rb, 256, 0, st>>>(J, njobs, vis_pref());
   } else {
-    const uint32_t n = (uint32_t)pixels + 1, nsb = cdiv(n, 1024);
-    cudaMemsetAsync(ent_cnt.p, 0, sizeof(uint32_t) * n, st);
-    cudaMemsetAsync(ent_cur.p, 0, sizeof(uint32_t) * pixels, st);
-    raster_kernel<true, false><<<rb, 256, 0, st>>>(J, njobs, vis_pref(), nullptr, 0);
-    scan_blocks_kernel<<<nsb, 1024, 0, st>>>(ent_cnt.as<uint32_t>(), n, ent_off.as<uint32_t>(),
+    // faces binned into 16 x 16 screen tiles, then per tile the pixels'
+    // depth-ordered entry lists
+    const uint32_t n = stiles + 1, nsb = cdiv(n, fb);
+    const uint32_t* ps = P + 4 * n1;
+    const uint32_t bcap = (uint32_t)std::min<size_t>(bin_cap, 0xffffffffu);
+    cudaMemsetAsync(tile_cnt.p, 0, sizeof(uint32_t) * n, st);
+    cudaMemsetAsync(tile_cur.p, 0, sizeof(uint32_t) * stiles, st);
+    bin_kernel<false><<<rb, 256, 0, st>>>(J, njobs, vis_pref(), ps, tile_cnt.as<uint32_t>(), nullptr,
+                                          nullptr, nullptr, 0);
+    scan_blocks_kernel<<<nsb, fb, 0, st>>>(tile_cnt.as<uint32_t>(), n, tile_off.as<uint32_t>(),
                                              scan.as<uint32_t>());
-    scan_add_kernel<<<nsb, 1024, 0, st>>>(ent_off.as<uint32_t>(), n, scan.as<uint32_t>(), nullptr);
-    raster_kernel<false, true><<<rb, 256, 0, st>>>(J, njobs, vis_pref(), ent.as<uint2>(),
-                                                   (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu));
-    entry_totals_kernel<<<cdiv(njobs, 128), 128, 0, st>>>(J, njobs);
+    scan_add_kernel<<<nsb, fb, 0, st>>>(tile_off.as<uint32_t>(), n, scan.as<uint32_t>(), nullptr);
+    bin_kernel<true><<<rb, 256, 0, st>>>(J, njobs, vis_pref(), ps, nullptr, tile_off.as<uint32_t>(),
+                                         tile_cur.as<uint32_t>(), bins.as<uint32_t>(), bcap);
+    if (stiles)
+      tile_kernel<<<std::min<uint32_t>(stiles, (uint32_t)C.num_sms * 8), 256, 0, st>>>(
+          J, njobs, ps, tile_off.as<uint32_t>(), bins.as<uint32_t>(), bcap, ent.as<uint2>(),
+          (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu), queue() + 1);
   }
   if (tiles) raylist_kernel<<<cdiv(tiles, 8), 256, 0, st>>>(J, njobs, P + 3 * n1, mode, tile_w);
-  prefix_kernel<<<1, 1024, 0, st>>>(J, njobs, 1, ray_pref());
+  prefix_kernel<<<1, fb, 0, st>>>(J, njobs, 1, ray_pref());
   return C.cuda(cudaGetLastError(), "stage (b) launch");
 }
 
@@ -456,6 +531,25 @@ int Batch::run() {
   return enqueue_all();
 }
 
+// Composited mode: whether the entry lists or the tile bins of the last run
+// needed more room than the layout gave them; if so the context's hints are
+// raised to the need (the next layout of a batch with ent_cap / bin_cap 0
+// sizes for it).
+bool Batch::overflowed(const std::vector<ViewCounters>& k) {
+  if (mode != VFR_MODE_COMPOSITED) return false;
+  uint64_t ents = 0, bns = 0;
+  for (const ViewCounters& x : k) {
+    ents += x.nentries;
+    bns += x.nbins;
+  }
+  const bool over = ents > ent_cap || bns > bin_cap;
+  if (over && ctx) {
+    ctx->ent_cap_hint = std::max<size_t>(ctx->ent_cap_hint, ents + ents / 8 + 1024);
+    ctx->bin_cap_hint = std::max<size_t>(ctx->bin_cap_hint, bns + bns / 8 + 1024);
+  }
+  return over;
+}
+
 int Batch::counters(std::vector<ViewCounters>& out) {
   Ctx& C = *ctx;
   out.resize(njobs);
@@ -464,6 +558,24 @@ int Batch::counters(std::vector<ViewCounters>& out) {
                   "counter read");
   if (!rc) rc = C.cuda(cudaStreamSynchronize(st()), "stream sync");
   return rc;
+}
+
+int serve_blocks_per_sm(int* n) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, serve_kernel<3>, 256, 0) == cudaSuccess
+             ? VFR_OK
+             : VFR_ERR_CUDA;
+}
+
+cudaError_t launch_serve(const ServeParams& sp, int grid, cudaStream_t st) {
+  serve_kernel<3><<<grid, 256, 0, st>>>(sp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_publish(SegDev* segs, ServeCtl* ctl, uint32_t seq, const JobDev* jobs,
+                           const uint32_t* ray_pref, uint32_t* done, uint32_t njobs,
+                           cudaStream_t st) {
+  publish_kernel<<<1, 256, 0, st>>>(segs, ctl, seq, jobs, ray_pref, done, njobs);
+  return cudaGetLastError();
 }
 
 }  // namespace vfr
@@ -849,10 +961,10 @@ int vfr_render(vfr_ctx* c, int id, const float* mv16, uint32_t W, uint32_t H, in
     std::vector<vfr::ViewCounters> k;
     if (!rc) rc = C.plain.counters(k);
     if (rc) return rc;
-    if (mode == VFR_MODE_COMPOSITED && k[0].nentries > C.plain.ent_cap) {
-      // entry lists overflowed: grow to the need and render again
+    if (C.plain.overflowed(k)) {
+      // entry lists or tile bins overflowed: grow to the need and render again
       C.plain.ent_cap = 0;
-      C.ent_cap_hint = k[0].nentries + k[0].nentries / 8 + 1024;
+      C.plain.bin_cap = 0;
       continue;
     }
     rc = copy_out(C, rgb8, rgba, steps, (size_t)W * H);
@@ -867,7 +979,7 @@ int vfr_render(vfr_ctx* c, int id, const float* mv16, uint32_t W, uint32_t H, in
     }
     return C.check_status(k[0].status, 0);
   }
-  return C.fail(VFR_ERR_DEVICE, "entry lists kept overflowing");
+  return C.fail(VFR_ERR_DEVICE, "entry lists or tile bins kept overflowing");
 }
 
 int vfr_render_device(vfr_ctx* c, int id, const float* mv16, uint32_t W, uint32_t H, int mode,
@@ -891,10 +1003,10 @@ int vfr_device_status(vfr_ctx* c, uint32_t* status) {
   int rc = C.plain.counters(k);
   if (rc) return rc;
   if (status) *status = k[0].status;
-  const uint32_t over = (C.plain.mode == VFR_MODE_COMPOSITED && k[0].nentries > C.plain.ent_cap);
+  const uint32_t over = C.plain.overflowed(k);
   if (over) {
     C.plain.ent_cap = 0;
-    C.ent_cap_hint = k[0].nentries + k[0].nentries / 8 + 1024;
+    C.plain.bin_cap = 0;
   }
   return C.check_status(k[0].status, over);
 }
@@ -999,11 +1111,7 @@ int vfr_batch_stats(vfr_batch* b, vfr_render_stats* per_job, uint32_t n) {
       fill_stats(k[j], b->b.jobs[j].nExt, &per_job[j]);
     }
   }
-  if (b->b.mode == VFR_MODE_COMPOSITED) {
-    uint64_t tot = 0;
-    for (auto& x : k) tot += x.nentries;
-    over = tot > b->b.ent_cap;
-  }
+  over = b->b.overflowed(k);
   return C.check_status(status, over);
 }
 

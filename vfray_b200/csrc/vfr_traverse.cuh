@@ -36,10 +36,16 @@ namespace vfr {
 // (rounded products and differences are symmetric), and its sum and slack
 // difference are the negations of the unswapped ones.  So the swap is a sign
 // flip of (c1, c2, sum - cr): applied by xor-ing the sign of cr into them.
-__device__ __forceinline__ bool exit_test(const float4& a, const float4& b, const float4& c,
-                                          float ox, float oy) {
+//
+// v2 = c - a is passed in: candidate 3's (r1 - r3) is the negation of
+// candidate 1's (r3 - r1), exact under round-to-nearest but for the sign of
+// a zero, and that sign cannot change the test: a zero v2 component only
+// changes the sign of a product that is zero, so of a sum or difference
+// that is zero; cr = 0 is skipped, and c1, c2 and the slack difference are
+// only compared with 0 and with 0x2b8cbccc, where -0 and +0 agree.
+__device__ __forceinline__ bool exit_test_v2(const float4& a, const float4& b, float v2x,
+                                             float v2y, float ox, float oy) {
   const float v1x = fsub(b.x, a.x), v1y = fsub(b.y, a.y);
-  const float v2x = fsub(c.x, a.x), v2y = fsub(c.y, a.y);
   const float cr = fsub(fmul(v1x, v2y), fmul(v1y, v2x));
   const bool skip = below_rdelta(cr);
   const float v0x = fsub(ox, a.x), v0y = fsub(oy, a.y);
@@ -51,6 +57,11 @@ __device__ __forceinline__ bool exit_test(const float4& a, const float4& b, cons
   const float c2s = __uint_as_float(__float_as_uint(c2) ^ sg);
   const float ds = __uint_as_float(__float_as_uint(d) ^ sg);
   return !skip && (c1s >= 0.0f) && (c2s >= 0.0f) && (ds <= __uint_as_float(0x2b8cbcccu));
+}
+
+__device__ __forceinline__ bool exit_test(const float4& a, const float4& b, const float4& c,
+                                          float ox, float oy) {
+  return exit_test_v2(a, b, fsub(c.x, a.x), fsub(c.y, a.y), ox, oy);
 }
 
 // x1, x2 or x3 by i (1, 2, otherwise 3), component by component (selects,
@@ -105,8 +116,8 @@ struct Ray {
   uint32_t t, f, p, iters;
   float ox, oy, zp;
   float ar, ag, ab, tr, lastZ;
-  // composited mode: this pixel's entry list and the last entry taken
-  uint32_t ea, en, dz_bits, de;
+  // composited mode: this pixel's entry list and the next entry to take
+  uint32_t ea, en, de;
   float exitZ;
   // served form: the job (its table entry lives in the server's arena) and
   // its completion flag
@@ -142,37 +153,23 @@ __device__ __forceinline__ void begin_segment(const JobDev& J, Ray& R, uint32_t 
   s_watch_saved[threadIdx.x] = 0xffffffffu;  // a new segment walks other states
 }
 
-// Composited mode: the next entry of the pixel in (depth, index) descending
-// order after the last one taken, skipping entries above the depth where the
-// previous segment left the mesh.  Returns false when the list is done.
+// Composited mode: the pixel's next entry in its list, which stage (b)
+// wrote in descending (depth, face) order, skipping entries above the depth
+// where the previous segment left the mesh.  Returns false when the list is
+// done.
 __device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev& J,
                                            Ray& R, bool first) {
-  for (;;) {
-    float bz = -INFINITY;
-    uint32_t be = 0, bzb = 0;
-    bool found = false;
-    const float dzl = __uint_as_float(R.dz_bits);
-    for (uint32_t k = 0; k < R.en; ++k) {
-      const uint2 q = J.ent[R.ea + k];
-      const float z = __uint_as_float(q.x);
-      const bool below = first || (z < dzl) || (z == dzl && q.y < R.de);
-      if (!below) continue;
-      if (!found || z > bz || (z == bz && q.y > be)) {
-        bz = z;
-        be = q.y;
-        bzb = q.x;
-        found = true;
-      }
-    }
-    if (!found) return false;
-    R.dz_bits = bzb;
-    R.de = be;
-    first = false;
-    if (bz > R.exitZ) continue;  // behind the ray already
-    const float4 p0 = J.planes[kPlaneStride * (size_t)be], p1 = J.planes[kPlaneStride * (size_t)be + 1];
-    begin_segment(J, R, be, bz, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
+  (void)first;
+  while (R.de < R.en) {
+    const uint2 q = J.ent[R.ea + R.de];
+    ++R.de;
+    const float z = __uint_as_float(q.x);
+    if (z > R.exitZ) continue;  // behind the ray already
+    const float4 p0 = J.planes[kPlaneStride * (size_t)q.y], p1 = J.planes[kPlaneStride * (size_t)q.y + 1];
+    begin_segment(J, R, q.y, z, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
     return true;
   }
+  return false;
 }
 
 __device__ __forceinline__ void finish_pixel(const JobDev& J, const Ray& R) {
@@ -296,9 +293,10 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   ++R.iters;
   uint32_t st = kContinue;
   if (kWatched) st = watched_step(P, R);
-  const bool h1 = exit_test(R.r1, R.r2, R.r3, R.ox, R.oy);
+  const float e13x = fsub(R.r3.x, R.r1.x), e13y = fsub(R.r3.y, R.r1.y);
+  const bool h1 = exit_test_v2(R.r1, R.r2, e13x, e13y, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
-  const bool h3 = exit_test(R.r3, R.r0, R.r1, R.ox, R.oy);
+  const bool h3 = exit_test_v2(R.r3, R.r0, -e13x, -e13y, R.ox, R.oy);
   const uint32_t i = h1 ? 1u : (h2 ? 2u : (h3 ? 3u : 0u));
   st = (st == kContinue && i == 0) ? kSegmentEnd : st;  // :353 no exit face
   const uint32_t ex = (R.f + i) & 3u;
@@ -421,15 +419,9 @@ __device__ __forceinline__ bool start_ray(const TraverseParams& P, const JobDev&
     return true;
   }
   R.ea = J.ent_off[R.p];
-  const uint32_t b1 = J.ent_off[R.p + 1];
-  R.en = b1 - R.ea;
+  R.en = J.ent_cnt[R.p];
   R.exitZ = INFINITY;
-  R.dz_bits = 0;
   R.de = 0;
-  if (b1 > J.ent_cap) {
-    status |= 16u;  // VFR_DEV_OVERFLOW: the caller renders again with room
-    return false;
-  }
   if (next_entry(P, J, R, true)) return true;
   finish_pixel(J, R);
   return false;
@@ -554,6 +546,19 @@ __device__ __forceinline__ void served_ray_done(const Ray& R, uint32_t status) {
   }
 }
 
+// A segment-table entry read through L2 only (ld.global.cg): entries are
+// 40 bytes, several to a cache line, and each is written (once per epoch)
+// after this launch may already have cached the line for an earlier entry.
+__device__ __forceinline__ SegDev load_seg(const SegDev* p) {
+  static_assert(sizeof(SegDev) == 40, "segment-table entry layout");
+  const unsigned long long* w = reinterpret_cast<const unsigned long long*>(p);
+  SegDev d;
+  unsigned long long* o = reinterpret_cast<unsigned long long*>(&d);
+#pragma unroll
+  for (int i = 0; i < 5; ++i) o[i] = __ldcg(w + i);
+  return d;
+}
+
 // The served form's persistent traversal: one long-lived launch whose warps
 // take rays from the published segments in order, oldest first, while the
 // host publishes new ones (requests admitted while this launch runs fold
@@ -573,7 +578,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) serve_kernel(ServeParams SP) 
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lt_mask = (1u << lane) - 1u;
   const uint32_t refill = P.refill ? P.refill : 1u;
-  uint32_t cur = SP.ctl->first;  // this warp's entry of the segment table
+  uint32_t cur = SP.first;  // this warp's entry of the segment table
   uint32_t idle_polls = 0;
   bool active = false;
   Ray R;
@@ -589,7 +594,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) serve_kernel(ServeParams SP) 
         while (cur < pub) {
           SegDev* sg = SP.segs + cur;
           const uint32_t b = atomicAdd(&sg->head, k);
-          const uint32_t n = sg->nrays;  // written before the entry was published
+          const uint32_t n = __ldcg(&sg->nrays);  // written before the entry was published
           if (b < n) {
             base = b;
             nr = n;
@@ -603,10 +608,11 @@ __global__ void __launch_bounds__(256, kMinBlocks) serve_kernel(ServeParams SP) 
       seg = __shfl_sync(0xffffffffu, seg, leader);
       base = __shfl_sync(0xffffffffu, base, leader);
       nr = __shfl_sync(0xffffffffu, nr, leader);
+      __syncwarp();  // the leader's acquire of the publication orders the lanes' reads
       if (seg != 0xffffffffu && !active) {
         const uint32_t g = base + __popc(idle & lt_mask);
         if (g < nr) {
-          const SegDev& sg = SP.segs[seg];
+          const SegDev sg = load_seg(SP.segs + seg);
           const uint32_t j = job_of(sg.ray_pref, sg.njobs, g);
           R.jp = sg.jobs + j;
           R.done = sg.done + j;

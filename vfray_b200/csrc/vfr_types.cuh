@@ -15,6 +15,7 @@ struct __align__(16) ViewCounters {
   uint32_t maxedge_bits;     // view maxEdgeLength (float bits, >= 0)
   uint32_t rays_done;        // served form: rays of this job finished so far
   uint32_t mm[8];            // orderable min x y z s, max x y z s (view set-up)
+  uint32_t nbins;            // composited: (face, screen tile) pairs of this job
 };
 
 // One job as the kernels see it (device memory, uploaded with the batch).
@@ -34,10 +35,10 @@ struct __align__(16) JobDev {
   uint4* bbox;               // per visible face
   int32_t* winner;           // W*H, reference mode
   uint32_t* rays;            // W*H capacity
-  uint32_t* ent_cnt;         // composited: W*H counts (batch arena)
-  uint32_t* ent_off;         // composited: offsets (batch arena, global)
-  uint32_t* ent_cur;
-  const uint2* ent;          // composited: the batch's entry arena (z bits, ext face)
+  uint32_t* ent_cnt;         // composited: W*H entry counts
+  uint32_t* ent_off;         // composited: W*H offsets of the pixels' lists in ent
+  const uint2* ent;          // composited: the batch's entry arena (z bits, ext face),
+                             // each pixel's list in descending (depth, face) order
   uint32_t ent_cap;          // its capacity in entries
   ViewCounters* ctr;
   uint8_t* rgb8;             // outputs (any may be null)
@@ -90,8 +91,7 @@ struct SegDev {
 struct ServeCtl {
   uint32_t published;        // entries of the segment table published in this epoch
   uint32_t status;           // VFR_DEV_QUEUE: an idle warp's bounded wait gave up
-  uint32_t first;            // the oldest entry with rays left when the launch starts
-  uint32_t pad;
+  uint32_t pad[2];
 };
 
 struct ServeParams {
@@ -100,6 +100,7 @@ struct ServeParams {
   ServeCtl* ctl;
   const volatile uint32_t* stop;  // mapped host memory: the host asks idle warps to leave
   uint32_t idle_limit;       // polls (about 1 us each) an idle warp makes before it gives up
+  uint32_t first;            // the oldest entry with rays left when the launch starts
 };
 
 }  // namespace vfr

@@ -1,8 +1,8 @@
 """Served form: a request loop with continuous batching over resident
 meshes (vfr_server_* in include/vfray.h).  Requests submitted from any
-thread are admitted by memory footprint, folded into batches of mixed meshes
-and image sizes, and run on two overlapping batch slots; each completed
-request carries its submit / start / done times."""
+thread are admitted by memory footprint and folded into one running
+persistent traversal launch, meshes and image sizes mixed; each completed
+request carries its submit / admission / done times."""
 from __future__ import annotations
 
 import ctypes as C
@@ -58,6 +58,12 @@ class Server:
             out = self._outs.pop(ticket, None)
         check(rc, None, "vfr_server_wait")
         return out, info.as_dict()
+
+    def set_idle(self, drain_idle_polls: int, linger_ms: int):
+        """The drain's bounded idle wait (polls of about 1 us) and how long
+        an idle drain runs before the server stops it."""
+        check(self.lib.vfr_server_set_idle(self.h, drain_idle_polls, linger_ms), None,
+              "vfr_server_set_idle")
 
     def stats(self) -> dict:
         s = ServerStats()
