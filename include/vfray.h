@@ -284,12 +284,12 @@ VFR_API int vfr_server_submit(vfr_server* s, const vfr_request* r, uint64_t* tic
  * out), fills info, forgets the ticket; returns the request's status. */
 VFR_API int vfr_server_wait(vfr_server* s, uint64_t ticket, int timeout_ms, vfr_request_info* info);
 VFR_API int vfr_server_stats(vfr_server* s, vfr_server_counters* out);
-/* Idle behaviour: the drain's bounded wait for new work (polls of about a
- * microsecond each, default 400000; when it runs out the drain sets
- * VFR_DEV_QUEUE, leaves, and is launched again with the next request) and
- * how long the worker lets an idle drain run before it stops it and starts
- * a new arena epoch (default 50 ms).  Applies from the next drain launch. */
-VFR_API int vfr_server_set_idle(vfr_server* s, uint32_t drain_idle_polls, uint32_t linger_ms);
+/* Idle behaviour: the drain's bounded wait for new work (microseconds,
+ * default 400000; when it runs out the drain sets VFR_DEV_QUEUE, leaves, and
+ * is launched again with the next request) and how long the worker lets an
+ * idle drain run before it stops it and starts a new arena epoch (default
+ * 50 ms).  Applies from the next drain launch. */
+VFR_API int vfr_server_set_idle(vfr_server* s, uint32_t drain_idle_us, uint32_t linger_ms);
 /* Drains the admitted and pending requests, then stops. */
 VFR_API void vfr_server_destroy(vfr_server* s);
 

@@ -133,7 +133,7 @@ def test_drain_idle_wait_is_bounded(renderer, meshes):
     bounded wait for work runs out: it records VFR_DEV_QUEUE and leaves, and
     the next request is served by a new launch."""
     with serve.Server(renderer, budget_bytes=4 << 30) as S:
-        S.set_idle(2000, 60000)  # about 2-4 ms of polls; the server never stops it
+        S.set_idle(2000, 60000)  # a 2 ms bounded wait; the server never stops it
         a = S.wait(S.submit(meshes[0], 64, 64))[1]
         deadline = time.time() + 10
         while S.stats()["queue_timeouts"] < 1 and time.time() < deadline:

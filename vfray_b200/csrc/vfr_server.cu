@@ -55,8 +55,8 @@ using vfr::JobSpec;
 
 constexpr uint32_t kMaxSegs = 8192;        // segment-table entries per epoch
 constexpr uint32_t kMaxFlags = 1u << 20;   // completion flags per epoch
-constexpr int kReserveCtas = 24;           // traversal CTAs left out for the preparation
-constexpr uint32_t kIdleLimit = 400000;    // default: drain polls (about 1 us each) before it gives up
+constexpr int kReserveDivisor = 2;        // traversal CTAs left out for the preparation: SMs / this
+constexpr uint32_t kIdleLimit = 400000;    // default: microseconds an idle drain waits for work
 constexpr double kLingerMs = 50.0;         // default: idle time before the worker stops the drain
 
 struct Seg;
@@ -151,7 +151,7 @@ struct vfr_server {
   vfr::SegDev* segs = nullptr;  // kMaxSegs entries
   vfr::ServeCtl* ctl = nullptr;
   uint32_t* flags = nullptr;    // mapped host memory, kMaxFlags completion flags
-  uint32_t* stop = nullptr;     // mapped host memory: ask the drain's idle warps to leave
+  uint32_t* stop = nullptr;     // pinned: [0] the stop word copied to the drain, [16] its status back
   cudaStream_t prep = nullptr, drain = nullptr, copy = nullptr;
   cudaEvent_t drain_done = nullptr;
   int drain_grid = 0;
@@ -192,6 +192,9 @@ struct vfr_server {
   bool admit();
   int launch_drain();
   void epoch_reset();
+  void send_stop();
+  bool stop_sent = false;
+  cudaEvent_t stop_copied = nullptr;  // the stop copy, ordered before the next launch's reset
   void fail_all(int rc);
 
 };
@@ -215,6 +218,7 @@ int vfr_server::start(uint64_t budget_bytes) {
   if (!rc) rc = X.cuda(cudaStreamCreateWithFlags(&drain, cudaStreamNonBlocking), "server streams");
   if (!rc) rc = X.cuda(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking), "server streams");
   if (!rc) rc = X.cuda(cudaEventCreateWithFlags(&drain_done, cudaEventDisableTiming), "server event");
+  if (!rc) rc = X.cuda(cudaEventCreateWithFlags(&stop_copied, cudaEventDisableTiming), "server event");
   // every resident mesh gets its distinct edges now (allocations and waits
   // are not allowed once the drain runs); their bytes count against the budget
   for (auto& m : X.meshes)
@@ -240,7 +244,7 @@ int vfr_server::start(uint64_t budget_bytes) {
   if (!rc)
     rc = X.cuda(cudaHostAlloc((void**)&flags, sizeof(uint32_t) * kMaxFlags, cudaHostAllocMapped),
                 "completion flags");
-  if (!rc) rc = X.cuda(cudaHostAlloc((void**)&stop, 256, cudaHostAllocMapped), "stop flag");
+  if (!rc) rc = X.cuda(cudaHostAlloc((void**)&stop, 256, cudaHostAllocDefault), "stop word");
   // pinned staging for every upload and image copy of the server's life:
   // a sixteenth of the budget, between 64 MB and 1 GB
   const size_t pool_cap =
@@ -253,7 +257,7 @@ int vfr_server::start(uint64_t budget_bytes) {
   *(volatile uint32_t*)stop = 0;
   int occ = 0;
   if (vfr::serve_blocks_per_sm(&occ) != VFR_OK) return X.fail(VFR_ERR_CUDA, "drain occupancy");
-  drain_grid = std::max(X.num_sms, occ * X.num_sms - kReserveCtas);
+  drain_grid = std::max(X.num_sms, occ * X.num_sms - X.num_sms / kReserveDivisor);
   rc = X.cuda(cudaMemsetAsync(ctl, 0, sizeof(vfr::ServeCtl), prep), "server control");
   if (!rc) rc = X.cuda(cudaStreamSynchronize(prep), "server start");
   return rc;
@@ -277,6 +281,7 @@ void vfr_server::release_device() {
   if (flags) cudaFreeHost(flags);
   if (stop) cudaFreeHost(stop);
   if (drain_done) cudaEventDestroy(drain_done);
+  if (stop_copied) cudaEventDestroy(stop_copied);
   for (cudaStream_t s : {prep, drain, copy})
     if (s) cudaStreamDestroy(s);
 }
@@ -296,12 +301,11 @@ int vfr_server::launch_drain() {
   SP.T.refill = X.tune.refill;
   SP.segs = segs;
   SP.ctl = ctl;
-  uint32_t* stop_dev = nullptr;
-  if (cudaHostGetDevicePointer((void**)&stop_dev, stop, 0) != cudaSuccess) return VFR_ERR_CUDA;
-  SP.stop = stop_dev;
   SP.idle_limit = idle_limit.load();
   SP.first = inflight.empty() ? seq : inflight.front()->seq;
-  *(volatile uint32_t*)stop = 0;
+  if (stop_sent && cudaStreamWaitEvent(drain, stop_copied, 0) != cudaSuccess) return VFR_ERR_CUDA;
+  stop_sent = false;
+  if (cudaMemsetAsync(&ctl->stop, 0, sizeof(uint32_t), drain) != cudaSuccess) return VFR_ERR_CUDA;
   if (vfr::launch_serve(SP, drain_grid, drain) != cudaSuccess) return VFR_ERR_CUDA;
   // the control word's status comes back with the launch's end
   if (cudaMemcpyAsync(stop + 16, &ctl->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, drain) !=
@@ -311,6 +315,17 @@ int vfr_server::launch_drain() {
   drain_running = true;
   ++launches;
   return VFR_OK;
+}
+
+// Asks the drain's idle warps to leave: the stop word goes to device memory
+// by a copy on the copy stream (the drain polls device memory only).
+void vfr_server::send_stop() {
+  if (stop_sent) return;
+  *(volatile uint32_t*)stop = 1u;
+  if (cudaMemcpyAsync(&ctl->stop, stop, sizeof(uint32_t), cudaMemcpyHostToDevice, copy) != cudaSuccess ||
+      cudaEventRecord(stop_copied, copy) != cudaSuccess)
+    cudaGetLastError();
+  stop_sent = true;
 }
 
 // A new epoch: the drain has left and nothing is in flight, so the arena,
@@ -548,7 +563,7 @@ void vfr_server::loop() {
   cudaSetDevice(C->device);
   for (;;) {
     if (fatal) {  // every request has failed: stop the drain and leave
-      *(volatile uint32_t*)stop = 1u;
+      if (drain_running) send_stop();
       if (!drain_running || cudaEventQuery(drain_done) != cudaErrorNotReady) break;
       std::this_thread::sleep_for(std::chrono::microseconds(50));
       continue;
@@ -587,7 +602,7 @@ void vfr_server::loop() {
                 std::chrono::duration<double, std::milli>(now - last_busy).count() > linger_ms.load())) {
       stopping = true;  // idle for a while (or shutting down): let the drain go
     }
-    if (stopping && inflight.empty() && drain_running) *(volatile uint32_t*)stop = 1u;
+    if (stopping && inflight.empty() && drain_running) send_stop();
     if (!progress) {
       if (busy || drain_running) {
         std::this_thread::sleep_for(std::chrono::microseconds(20));
@@ -685,9 +700,9 @@ int vfr_server_wait(vfr_server* s, uint64_t ticket, int timeout_ms, vfr_request_
   return st;
 }
 
-int vfr_server_set_idle(vfr_server* s, uint32_t drain_idle_polls, uint32_t linger_ms) {
-  if (!s || drain_idle_polls == 0) return VFR_ERR_INVALID;
-  s->idle_limit = drain_idle_polls;
+int vfr_server_set_idle(vfr_server* s, uint32_t drain_idle_us, uint32_t linger_ms) {
+  if (!s || drain_idle_us == 0) return VFR_ERR_INVALID;
+  s->idle_limit = drain_idle_us;
   s->linger_ms = (double)linger_ms;
   return VFR_OK;
 }

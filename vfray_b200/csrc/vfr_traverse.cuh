@@ -559,6 +559,34 @@ __device__ __forceinline__ SegDev load_seg(const SegDev* p) {
   return d;
 }
 
+// The same for every lane of the warp whose ray ended in this pass (fin),
+// aggregated per job: one fence and one atomic per job and pass.  Called by
+// the whole warp.  The lanes' pixel writes are ordered before the leader's
+// fence by __syncwarp, and the leader's count after its fence.
+__device__ __forceinline__ void served_rays_done(const Ray& R, bool fin, uint32_t status) {
+  const uint32_t finm = __ballot_sync(0xffffffffu, fin);
+  if (!finm) return;
+  if (fin) {
+    const uint32_t peers = __match_any_sync(finm, (unsigned long long)(uintptr_t)R.jp);
+    // steps as two 16-bit halves, so the 32-bit warp sums cannot overflow
+    const uint32_t lo = __reduce_add_sync(peers, R.iters & 0xffffu);
+    const uint32_t hi = __reduce_add_sync(peers, R.iters >> 16);
+    const uint32_t st = __reduce_or_sync(peers, status);
+    __syncwarp(peers);
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) {
+      ViewCounters* c = R.jp->ctr;
+      atomicAdd(&c->steps, ((unsigned long long)hi << 16) + lo);
+      if (st) atomicOr(&c->status, st);
+      __threadfence();
+      const uint32_t n = atomicAdd(&c->rays_done, (uint32_t)__popc(peers)) + __popc(peers);
+      if (n == *(volatile const uint32_t*)&c->nrays) {
+        __threadfence_system();
+        *(volatile uint32_t*)R.done = 1u;
+      }
+    }
+  }
+}
+
 // The served form's persistent traversal: one long-lived launch whose warps
 // take rays from the published segments in order, oldest first, while the
 // host publishes new ones (requests admitted while this launch runs fold
@@ -567,9 +595,10 @@ __device__ __forceinline__ SegDev load_seg(const SegDev* p) {
 // the entry is drained.  Jobs of either mode may be mixed (kMode 2 per job).
 // A warp with nothing to do polls for newly published segments: it leaves
 // when the host's stop flag is set, or sets VFR_DEV_QUEUE in the control
-// word and leaves when idle_limit polls found nothing -- a bounded wait, so
-// a launch never outlives its work by more than about idle_limit
-// microseconds.  The host relaunches it when work arrives after it left.
+// word and leaves when it has found nothing for idle_limit microseconds
+// (%globaltimer) -- a bounded wait, so a launch never outlives its work by
+// much more than that.  The host relaunches it when work arrives after it
+// left.
 template <int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) serve_kernel(ServeParams SP) {
   const TraverseParams& P = SP.T;
@@ -579,36 +608,49 @@ __global__ void __launch_bounds__(256, kMinBlocks) serve_kernel(ServeParams SP) 
   const uint32_t lt_mask = (1u << lane) - 1u;
   const uint32_t refill = P.refill ? P.refill : 1u;
   uint32_t cur = SP.first;  // this warp's entry of the segment table
-  uint32_t idle_polls = 0;
+  // Polling costs: a warp with nothing to do polls the publication count and
+  // the stop word (device memory) with plain loads by one lane, backing off
+  // from 256 ns to 256 us between polls, and a warp whose claim found
+  // nothing while some of its lanes still walk waits 32 passes before it
+  // tries again -- thousands of warps polling back to back would make those
+  // L2 lines hot spots that slow everything, the preparation kernels beside
+  // this launch included.
+  unsigned long long idle_since = 0;  // %globaltimer (ns) when the warp found nothing (0: busy)
+  uint32_t backoff = 256, quiet = 0;
   bool active = false;
   Ray R;
   for (;;) {
     const uint32_t idle = __ballot_sync(0xffffffffu, !active);
     uint32_t seg = 0xffffffffu;
-    if (idle && ((uint32_t)__popc(idle) >= refill || idle == 0xffffffffu)) {
+    if (quiet) --quiet;
+    if (idle && (idle == 0xffffffffu || ((uint32_t)__popc(idle) >= refill && quiet == 0))) {
       const uint32_t leader = __ffs(idle) - 1u, k = __popc(idle);
       uint32_t base = 0, nr = 0;
       if (lane == leader) {
-        uint32_t pub;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(pub) : "l"(&SP.ctl->published));
-        while (cur < pub) {
-          SegDev* sg = SP.segs + cur;
-          const uint32_t b = atomicAdd(&sg->head, k);
-          const uint32_t n = __ldcg(&sg->nrays);  // written before the entry was published
-          if (b < n) {
-            base = b;
-            nr = n;
-            seg = cur;
-            break;
+        const uint32_t pub = *(volatile const uint32_t*)&SP.ctl->published;
+        if (cur < pub) {
+          // with the publisher's release, the entries below pub are visible
+          __threadfence();
+          while (cur < pub) {
+            SegDev* sg = SP.segs + cur;
+            const uint32_t b = atomicAdd(&sg->head, k);
+            const uint32_t n = __ldcg(&sg->nrays);  // written before the entry was published
+            if (b < n) {
+              base = b;
+              nr = n;
+              seg = cur;
+              break;
+            }
+            ++cur;  // drained: the next entry
           }
-          ++cur;  // drained: the next entry
         }
       }
       cur = __shfl_sync(0xffffffffu, cur, leader);
       seg = __shfl_sync(0xffffffffu, seg, leader);
       base = __shfl_sync(0xffffffffu, base, leader);
       nr = __shfl_sync(0xffffffffu, nr, leader);
-      __syncwarp();  // the leader's acquire of the publication orders the lanes' reads
+      __syncwarp();  // the leader's fence after the publication orders the lanes' reads
+      if (seg == 0xffffffffu) quiet = 32;
       if (seg != 0xffffffffu && !active) {
         const uint32_t g = base + __popc(idle & lt_mask);
         if (g < nr) {
@@ -624,40 +666,54 @@ __global__ void __launch_bounds__(256, kMinBlocks) serve_kernel(ServeParams SP) 
     }
     if (!__any_sync(0xffffffffu, active)) {
       if (seg == 0xffffffffu) {  // nothing published to take: wait, boundedly
-        if (*SP.stop) break;
-        if (++idle_polls > SP.idle_limit) {
+        // lane 0's reads decide for the warp, which leaves together
+        unsigned long long now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        now = __shfl_sync(0xffffffffu, now, 0);
+        const uint32_t stop = lane == 0 ? *(volatile const uint32_t*)&SP.ctl->stop : 0u;
+        if (__shfl_sync(0xffffffffu, stop, 0)) break;
+        if (!idle_since) {
+          idle_since = now;
+        } else if (now - idle_since > 1000ull * SP.idle_limit) {
           if (lane == 0) atomicOr(&SP.ctl->status, 8u);  // VFR_DEV_QUEUE
           break;
         }
-        __nanosleep(1000);
+        __nanosleep(backoff);
+        backoff = min(2u * backoff, 262144u);
       }
       continue;
     }
-    idle_polls = 0;
-    if (!active) continue;
-    uint32_t res;
-    if (R.iters + 2u <= R.watch) {
-      res = step<false, true>(P, S, R);
-      if (res == kContinue) res = step<false, true>(P, S, R);
-    } else {
-      res = step<true, true>(P, S, R);
-    }
-    if (res == kContinue) continue;
-    uint32_t status = 0;
-    if (res == kSegmentEnd) {
-      if (R.jp->mode == 1) {
-        R.exitZ = R.lastZ;
-        if (next_entry(P, *R.jp, R, false)) continue;
+    idle_since = 0;
+    backoff = 256;
+    // every lane goes on to served_rays_done, which syncs the whole warp
+    uint32_t res = kContinue;
+    if (active) {
+      if (R.iters + 2u <= R.watch) {
+        res = step<false, true>(P, S, R);
+        if (res == kContinue) res = step<false, true>(P, S, R);
+      } else {
+        res = step<true, true>(P, S, R);
       }
-      finish_pixel(*R.jp, R);
-    } else if (res == kCycle || res == kCap) {
-      status = res == kCycle ? 32u : 2u;
-      finish_pixel(*R.jp, R);
-    } else {
-      status = 4u;
     }
-    served_ray_done(R, status);
-    active = false;
+    uint32_t status = 0;
+    bool fin = false;
+    if (active && res != kContinue) {
+      fin = true;
+      if (res == kSegmentEnd) {
+        if (R.jp->mode == 1) {
+          R.exitZ = R.lastZ;
+          fin = !next_entry(P, *R.jp, R, false);
+        }
+        if (fin) finish_pixel(*R.jp, R);
+      } else if (res == kCycle || res == kCap) {
+        status = res == kCycle ? 32u : 2u;
+        finish_pixel(*R.jp, R);
+      } else {
+        status = 4u;
+      }
+    }
+    served_rays_done(R, fin, status);
+    active = active && !fin;
   }
 }
 

@@ -91,15 +91,15 @@ struct SegDev {
 struct ServeCtl {
   uint32_t published;        // entries of the segment table published in this epoch
   uint32_t status;           // VFR_DEV_QUEUE: an idle warp's bounded wait gave up
-  uint32_t pad[2];
+  uint32_t stop;             // the host asks idle warps to leave (copied in while the drain runs)
+  uint32_t pad;
 };
 
 struct ServeParams {
   TraverseParams T;          // tables, step cap, refill (jobs, ray_pref, queue unused)
   SegDev* segs;
   ServeCtl* ctl;
-  const volatile uint32_t* stop;  // mapped host memory: the host asks idle warps to leave
-  uint32_t idle_limit;       // polls (about 1 us each) an idle warp makes before it gives up
+  uint32_t idle_limit;       // microseconds an idle warp waits for new work before it gives up
   uint32_t first;            // the oldest entry with rays left when the launch starts
 };
 

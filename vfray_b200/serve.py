@@ -59,10 +59,10 @@ class Server:
         check(rc, None, "vfr_server_wait")
         return out, info.as_dict()
 
-    def set_idle(self, drain_idle_polls: int, linger_ms: int):
-        """The drain's bounded idle wait (polls of about 1 us) and how long
-        an idle drain runs before the server stops it."""
-        check(self.lib.vfr_server_set_idle(self.h, drain_idle_polls, linger_ms), None,
+    def set_idle(self, drain_idle_us: int, linger_ms: int):
+        """The drain's bounded idle wait (microseconds) and how long an
+        idle drain runs before the server stops it."""
+        check(self.lib.vfr_server_set_idle(self.h, drain_idle_us, linger_ms), None,
               "vfr_server_set_idle")
 
     def stats(self) -> dict:
