@@ -46,7 +46,11 @@ extern "C" {
  * abandons the rest of a face (vfRayKernelCPU.cc:359-365), is refused at
  * upload instead (VFR_ERR_MESH). */
 #define VFR_DEV_STEP_CAP 2u   /* a ray hit the per-ray step cap (VFR_OPT_STEP_CAP) */
-#define VFR_DEV_RANGE 4u      /* an id read on the device was out of range */
+#define VFR_DEV_RANGE 4u      /* an id read on the device was out of range: reported by the
+                                 checked build (libvfray_b200_checked.so, -DVFR_CHECKED),
+                                 which compares every id a kernel reads with the extent it
+                                 indexes; the product build relies on the upload's
+                                 validation and does not compare */
 #define VFR_DEV_QUEUE 8u      /* a bounded wait of the served kernel for work gave up */
 #define VFR_DEV_OVERFLOW 16u  /* an entry list exceeded its capacity */
 #define VFR_DEV_CYCLE 32u     /* a ray's walk came back to a (tet, entry face) state it had

@@ -47,3 +47,18 @@ def test_missing_library_fails_loudly(tmp_path):
             _lib.load(str(tmp_path / "nope.so"))
     finally:
         _lib._LIB = old
+
+
+def test_checked_build_alone_has_its_test_hook():
+    """The checked build (-DVFR_CHECKED) is built beside the product library
+    and exports the same entry points plus its test hook, which the product
+    library does not have."""
+    import ctypes
+
+    path = os.path.join(ROOT, "vfray_b200", "libvfray_b200_checked.so")
+    assert os.path.exists(path), "build it with `make -C vfray_b200 checked`"
+    checked = ctypes.CDLL(path)
+    for n in declared():
+        assert hasattr(checked, n), n
+    assert hasattr(checked, "vfr_checked_set_id")
+    assert not hasattr(vb.load(), "vfr_checked_set_id")

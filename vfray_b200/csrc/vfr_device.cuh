@@ -15,6 +15,26 @@ namespace vfr {
 
 constexpr double kRDelta = 1e-12;  // vfRayKernelCPU.h:28 (a double)
 
+// The checked build (`make checked`: -DVFR_CHECKED) compares every id a
+// kernel reads from memory with the extent of the array it is about to
+// index: the mesh's tet, vertex and neighbour ids, and the visible-face,
+// bin, ray and entry ids the stages write for one another.  A bad id sets
+// VFR_DEV_RANGE in its job's status and the access is skipped (the face
+// counts as invisible, the pixel or the ray is dropped), so a corrupt input
+// or a stage bug shows as a status instead of a fault.  The product build
+// leaves the checks out: mesh ids are validated when the mesh is uploaded,
+// and the stages' ids are in range by construction.
+#ifdef VFR_CHECKED
+constexpr bool kChecked = true;
+#else
+constexpr bool kChecked = false;
+#endif
+constexpr uint32_t kDevRange = 4u;  // VFR_DEV_RANGE
+
+__host__ __device__ __forceinline__ bool id_bad(uint32_t id, uint32_t n) {
+  return kChecked && id >= n;
+}
+
 // Walk record of a tet, 32 bytes: the 4 neighbour ids (the conTet row, self
 // = boundary) and, per face f, one packed word q[f] describing the neighbour
 // n across f: bits 0-26 the id of n's vertex opposite the shared face (the

@@ -7,10 +7,22 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "vfr_host.h"
 #include "vfr_types.cuh"
 
 namespace vfr {
+
+// A named NVTX range over a host call or stage, for Nsight timelines and
+// ncu's --nvtx filters (header-only NVTX 3: a no-op unless a tool is
+// attached).
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
 
 // Grow-only device buffer, or a piece of an Arena (owned = false: never
 // freed by the buffer).

@@ -159,6 +159,10 @@ __global__ void __launch_bounds__(256) view_maxedge_kernel(const JobDev* __restr
   float best = 0.0f;
   for (uint32_t e = lb * blockDim.x + threadIdx.x; e < J.nEdges; e += nb * blockDim.x) {
     const uint2 ed = __ldg(J.edges + e);
+    if (id_bad(ed.x, J.nV) || id_bad(ed.y, J.nV)) {
+      atomicOr(&J.ctr->status, kDevRange);
+      continue;
+    }
     const float4 a = J.vview[ed.x], b = J.vview[ed.y];
     const float e0 = fsub(a.x, b.x), e1 = fsub(a.y, b.y), e2 = fsub(a.z, b.z);
     const float len = __fsqrt_rn(fadd(fadd(fmul(e0, e0), fmul(e1, e1)), fmul(e2, e2)));
@@ -204,7 +208,14 @@ __global__ void __launch_bounds__(1024) visible_kernel(const JobDev* __restrict_
   int vis = 0;
   if (e < J.nExt) {
     const uint2 tf = J.extf[e];
-    const uint4 id = J.tet[tf.x];
+    bool bad = id_bad(tf.x, J.nT);
+    uint4 id = J.tet[bad ? 0u : tf.x];
+    bad = bad || id_bad(id.x, J.nV) || id_bad(id.y, J.nV) || id_bad(id.z, J.nV) ||
+          id_bad(id.w, J.nV);
+    if (bad) {
+      id = make_uint4(0u, 0u, 0u, 0u);
+      atomicOr(&J.ctr->status, kDevRange);
+    }
     const float4 v0 = J.vert[sel4(id, tf.y & 3u)];
     const float4 v1 = J.vert[sel4(id, (tf.y + 1) & 3u)];
     const float4 v2 = J.vert[sel4(id, (tf.y + 2) & 3u)];
@@ -212,7 +223,7 @@ __global__ void __launch_bounds__(1024) visible_kernel(const JobDev* __restrict_
     Plane P;
     face_plane(v0, v1, v2, P);
     const float faceZ = plane_eval(op.x, op.y, P.zx, P.zy, P.zz);
-    if (faceZ < op.z) P.sx = -1.0f;  // :128 invisible sentinel
+    if (faceZ < op.z || bad) P.sx = -1.0f;  // :128 invisible sentinel
     vis = (P.sx != -1.0f);
     float4* pl = J.planes + kPlaneStride * (size_t)e;
     pl[0] = make_float4(P.zx, P.zy, P.zz, P.sx);
@@ -354,6 +365,10 @@ __global__ void __launch_bounds__(256) raster_kernel(const JobDev* __restrict__ 
     const uint32_t i = g - vpref[j];
     const uint32_t W = J.W, H = J.H;
     const uint32_t e = J.vis_ext[i];
+    if (id_bad(e, J.nExt)) {
+      if (lane == 0) atomicOr(&J.ctr->status, kDevRange);
+      continue;
+    }
     // the face's plane and vertex xy, written by stage (a): one dependent
     // load after the visible list instead of the face -> tet -> vertex chain
     const float4* pl = J.planes + kPlaneStride * (size_t)e;
@@ -430,8 +445,12 @@ __global__ void __launch_bounds__(256) bin_kernel(const JobDev* __restrict__ job
       j = job_of(vpref, njobs, g);
       const JobDev& J = jobs[j];
       const uint32_t i = g - vpref[j];
-      const float4* pl = J.planes + kPlaneStride * (size_t)J.vis_ext[i];
-      const uint4 b = face_box(pl[1], pl[2], J.W, J.H);
+      const uint32_t e = J.vis_ext[i];
+      const bool bad = id_bad(e, J.nExt);
+      if (bad) atomicOr(&J.ctr->status, kDevRange);
+      const float4* pl = J.planes + kPlaneStride * (size_t)(bad ? 0u : e);
+      uint4 b = face_box(pl[1], pl[2], J.W, J.H);
+      if (bad) b = make_uint4(1u, 1u, 0u, 0u);  // an empty box: no tiles
       if (!kFill) J.bbox[i] = b;
       const uint32_t xe = min(b.z, J.W - 1), ye = min(b.w, J.H - 1);
       if (b.x <= xe && b.y <= ye) {
@@ -508,12 +527,18 @@ __global__ void __launch_bounds__(256) tile_kernel(const JobDev* __restrict__ jo
     auto stage = [&](uint32_t c) {  // faces c .. c+255 of the bin into shared memory
       __syncthreads();
       if (c + tid < b1) {
-        const uint32_t i = bins[c + tid];
-        const uint32_t e = J.vis_ext[i];
+        uint32_t i = bins[c + tid];
+        bool bad = id_bad(i, J.ctr->nvis);
+        uint32_t e = J.vis_ext[bad ? 0u : i];
+        bad = bad || id_bad(e, J.nExt);
+        if (bad) {
+          i = e = 0;
+          atomicOr(&J.ctr->status, kDevRange);
+        }
         const float4* pl = J.planes + kPlaneStride * (size_t)e;
         const float4 p0 = pl[0], p1 = pl[1], p2 = pl[2];
         TileFace f;
-        f.box = J.bbox[i];
+        f.box = bad ? make_uint4(1u, 1u, 0u, 0u) : J.bbox[i];  // bad: covers nothing
         f.E = entry_edges(make_float4(p1.z, p1.w, 0.0f, 0.0f), make_float4(p2.x, p2.y, 0.0f, 0.0f),
                           make_float4(p2.z, p2.w, 0.0f, 0.0f));
         f.zx = p0.x;

@@ -747,6 +747,7 @@ int vfr_profile_read(vfr_ctx* c, float* ms3, int cap, int* count) {
 }
 
 int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
+  vfr::Range nvtx("vfr_tables_upload");
   CTX_OR_FAIL(c);
   if (!tf) return C.fail(VFR_ERR_INVALID, "transfer function is NULL");
   std::vector<float> ref;
@@ -780,6 +781,7 @@ int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
 int vfr_mesh_upload(vfr_ctx* c, const float* vert4, uint32_t nV, const uint32_t* tet4,
                     const uint32_t* con4, uint32_t nT, const uint32_t* extf2, uint32_t nExt,
                     float maxEdge, float maxZ, float minZ, int* mesh_id) {
+  vfr::Range nvtx("vfr_mesh_upload");
   CTX_OR_FAIL(c);
   if (!vert4 || !tet4 || !con4 || (!extf2 && nExt) || !mesh_id || nV == 0 || nT == 0)
     return C.fail(VFR_ERR_INVALID, "mesh arrays missing or empty");
@@ -852,6 +854,7 @@ int vfr_mesh_bytes(vfr_ctx* c, int id, uint64_t* bytes) {
 }
 
 int vfr_find_visible(vfr_ctx* c, int id, uint32_t* num_vis, uint32_t* visExt, float* faceData) {
+  vfr::Range nvtx("vfr_find_visible");
   CTX_OR_FAIL(c);
   Mesh* m = C.mesh(id);
   if (!m) return C.fail(VFR_ERR_STATE, "unknown mesh id");
@@ -881,6 +884,7 @@ int vfr_find_visible(vfr_ctx* c, int id, uint32_t* num_vis, uint32_t* visExt, fl
 }
 
 int vfr_project(vfr_ctx* c, int id, uint32_t W, uint32_t H, uint32_t* bbox, int32_t* writer) {
+  vfr::Range nvtx("vfr_project");
   CTX_OR_FAIL(c);
   Mesh* m = C.mesh(id);
   if (!m || C.stage < 1 || !C.plain.njobs || C.plain.specs[0].mesh != id)
@@ -907,6 +911,7 @@ int vfr_project(vfr_ctx* c, int id, uint32_t W, uint32_t H, uint32_t* bbox, int3
 
 int vfr_traverse(vfr_ctx* c, int id, uint8_t* rgb8, float* rgba, uint32_t* steps,
                  vfr_render_stats* stats) {
+  vfr::Range nvtx("vfr_traverse");
   CTX_OR_FAIL(c);
   Mesh* m = C.mesh(id);
   if (!m || C.stage < 2 || !C.plain.njobs || C.plain.specs[0].mesh != id)
@@ -955,6 +960,7 @@ static int render_one(Ctx& C, int id, const float* mv16, uint32_t W, uint32_t H,
 
 int vfr_render(vfr_ctx* c, int id, const float* mv16, uint32_t W, uint32_t H, int mode,
                uint8_t* rgb8, float* rgba, uint32_t* steps, vfr_render_stats* stats) {
+  vfr::Range nvtx("vfr_render");
   CTX_OR_FAIL(c);
   for (int attempt = 0; attempt < 4; ++attempt) {
     int rc = render_one(C, id, mv16, W, H, mode, true, nullptr, nullptr, nullptr, true);
@@ -984,6 +990,7 @@ int vfr_render(vfr_ctx* c, int id, const float* mv16, uint32_t W, uint32_t H, in
 
 int vfr_render_device(vfr_ctx* c, int id, const float* mv16, uint32_t W, uint32_t H, int mode,
                       uint8_t* rgb8_dev, float* rgba_dev, uint32_t* steps_dev, int32_t* writer_dev) {
+  vfr::Range nvtx("vfr_render_device");
   CTX_OR_FAIL(c);
   int rc = render_one(C, id, mv16, W, H, mode, false, rgb8_dev, (float4*)rgba_dev, steps_dev, false);
   if (!rc && writer_dev && mode == VFR_MODE_REF)
@@ -1036,6 +1043,7 @@ void vfr_batch_destroy(vfr_batch* b) {
 }
 
 int vfr_batch_set_jobs(vfr_batch* b, const vfr_job* jobs, uint32_t n, int mode) {
+  vfr::Range nvtx("vfr_batch_set_jobs");
   if (!b) return VFR_ERR_INVALID;
   if (!b->owner) return VFR_ERR_STATE;
   Ctx& C = b->owner->impl;
@@ -1063,6 +1071,7 @@ int vfr_batch_set_jobs(vfr_batch* b, const vfr_job* jobs, uint32_t n, int mode) 
 }
 
 int vfr_batch_capture(vfr_batch* b) {
+  vfr::Range nvtx("vfr_batch_capture");
   if (!b || !b->b.njobs) return VFR_ERR_STATE;
   if (!b->owner) return VFR_ERR_STATE;
   Ctx& C = b->owner->impl;
@@ -1072,6 +1081,7 @@ int vfr_batch_capture(vfr_batch* b) {
 }
 
 int vfr_batch_run(vfr_batch* b) {
+  vfr::Range nvtx("vfr_batch_run");
   if (!b || !b->b.njobs) return VFR_ERR_STATE;
   if (!b->owner) return VFR_ERR_STATE;
   Ctx& C = b->owner->impl;
@@ -1129,6 +1139,7 @@ int vfr_batch_output(vfr_batch* b, uint32_t job, uint8_t** rgb8_dev, float** rgb
 // traversal register budget, refill threshold, traversal CTAs per SM, ray
 // tile shape, stage (b) warps per SM -- and keeps the fastest on the context.
 int vfr_batch_autotune(vfr_batch* b, int reps, vfr_tuning* out) {
+  vfr::Range nvtx("vfr_batch_autotune");
   if (!b || !b->b.njobs) return VFR_ERR_STATE;
   if (!b->owner) return VFR_ERR_STATE;
   Ctx& C = b->owner->impl;
@@ -1205,6 +1216,7 @@ int vfr_batch_autotune(vfr_batch* b, int reps, vfr_tuning* out) {
 }
 
 int vfr_batch_set_cameras(vfr_batch* b, const float* mv16, uint32_t n) {
+  vfr::Range nvtx("vfr_batch_set_cameras");
   if (!b || !b->b.njobs) return VFR_ERR_STATE;
   if (!b->owner) return VFR_ERR_STATE;
   Ctx& C = b->owner->impl;
@@ -1228,6 +1240,7 @@ int vfr_batch_set_cameras(vfr_batch* b, const float* mv16, uint32_t n) {
 }
 
 int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host, uint32_t* steps_host) {
+  vfr::Range nvtx("vfr_batch_read");
   if (!b || !b->b.njobs) return VFR_ERR_STATE;
   if (!b->owner) return VFR_ERR_STATE;
   Ctx& C = b->owner->impl;
@@ -1277,5 +1290,30 @@ int vfr_batch_scratch_bytes(vfr_batch* b, uint64_t* bytes) {
   *bytes = b->b.scratch_bytes;
   return VFR_OK;
 }
+
+#ifdef VFR_CHECKED
+// Test hook of the checked build only (declared in no header: the product
+// library does not have it).  Overwrites one id of a resident mesh on the
+// device, past the validation at upload, so that a test can show the range
+// checks turning it into VFR_DEV_RANGE.  what: 0 = a neighbour id of a walk
+// record (index = 4 tet + face), 1 = a vertex id of the tet array (index =
+// 4 tet + corner), 2 = the tet id of an external face (index = the face).
+__attribute__((visibility("default"))) int vfr_checked_set_id(vfr_ctx* c, int id, int what,
+                                                              uint64_t index, uint32_t value) {
+  CTX_OR_FAIL(c);
+  Mesh* m = C.mesh(id);
+  if (!m) return C.fail(VFR_ERR_STATE, "unknown mesh id");
+  uint32_t* dst = nullptr;
+  if (what == 0 && index < 4ull * m->nT)
+    dst = reinterpret_cast<uint32_t*>(m->walk + index / 4) + index % 4;
+  else if (what == 1 && index < 4ull * m->nT)
+    dst = reinterpret_cast<uint32_t*>(m->tet) + index;
+  else if (what == 2 && index < m->nExt)
+    dst = reinterpret_cast<uint32_t*>(m->extf + index);
+  if (!dst) return C.fail(VFR_ERR_INVALID, "checked_set_id: no such id");
+  if (int rc = C.cuda(cudaDeviceSynchronize(), "checked_set_id")) return rc;
+  return C.cuda(cudaMemcpy(dst, &value, sizeof value, cudaMemcpyHostToDevice), "checked_set_id");
+}
+#endif
 
 }  // extern "C"

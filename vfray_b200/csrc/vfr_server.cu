@@ -212,6 +212,7 @@ uint64_t vfr_server::footprint(const vfr_request& r) const {
 }
 
 int vfr_server::start(uint64_t budget_bytes) {
+  vfr::Range nvtx("vfr_server start");
   vfr::Ctx& X = *C;
   budget = budget_bytes;
   int rc = X.cuda(cudaStreamCreateWithFlags(&prep, cudaStreamNonBlocking), "server streams");
@@ -291,6 +292,7 @@ void vfr_server::release_device() {
 // previous launch took were all finished before its warps left (a warp
 // leaves only when its lanes are idle), so the heads stand as they are.
 int vfr_server::launch_drain() {
+  vfr::Range nvtx("vfr_server drain launch");
   vfr::Ctx& X = *C;
   vfr::ServeParams SP;
   std::memset(&SP, 0, sizeof SP);
@@ -331,6 +333,7 @@ void vfr_server::send_stop() {
 // A new epoch: the drain has left and nothing is in flight, so the arena,
 // the segment table and the flags start again from the beginning.
 void vfr_server::epoch_reset() {
+  vfr::Range nvtx("vfr_server epoch reset");
   arena.off = 0;
   seq = 0;
   std::memset(flags, 0, sizeof(uint32_t) * flags_used);
@@ -367,6 +370,7 @@ void vfr_server::fail_all(int rc) {
 // the image to the request, which is then done.  Returns whether anything
 // moved.
 bool vfr_server::poll_completions() {
+  vfr::Range nvtx("vfr_server completions");
   bool progress = false;
   const volatile uint32_t* f = flags;
   for (Seg* g : inflight)
@@ -449,6 +453,7 @@ bool vfr_server::poll_completions() {
 // preparation stream and publishes it to the drain.  Returns whether a
 // segment was formed.
 bool vfr_server::admit() {
+  vfr::Range nvtx("vfr_server admit");
   if (stopping || fatal) return false;
   std::vector<Req*> take;
   uint64_t bytes = 0;

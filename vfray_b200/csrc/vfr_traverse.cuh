@@ -110,6 +110,7 @@ struct Ray {
   const WalkRec* walk;         // this job's mesh and view vertices
   const float4* vert;
   uint32_t j, nT;
+  uint32_t nV;                 // checked build: vertex ids are compared with it
   uint32_t watch;              // min(kWatchSteps, step cap): longer rays are checked
   double rmaxEdge;             // 1 / maxEdgeLength, correctly rounded (div_by)
   uint32_t cbi;                // colorBack: its transfer-function entry
@@ -135,13 +136,18 @@ __device__ __forceinline__ WalkRec ldg_walk(const WalkRec* w, uint32_t t) {
   return r;
 }
 
-// Start a segment at external face e with entry depth zp (:256-279).
-__device__ __forceinline__ void begin_segment(const JobDev& J, Ray& R, uint32_t e, float zp,
+// Start a segment at external face e (in range: the caller read its plane)
+// with entry depth zp (:256-279).  False (checked build only): the face's
+// tet or one of its vertex ids is out of range, and nothing was loaded.
+__device__ __forceinline__ bool begin_segment(const JobDev& J, Ray& R, uint32_t e, float zp,
                                               float sp) {
   const uint2 tf = __ldg(J.extf + e);
+  if (id_bad(tf.x, J.nT)) return false;
   R.t = tf.x;
   R.f = tf.y;
   const uint4 id = __ldg(J.tet + R.t);
+  if (id_bad(id.x, J.nV) || id_bad(id.y, J.nV) || id_bad(id.z, J.nV) || id_bad(id.w, J.nV))
+    return false;
   R.w = ldg_walk(R.walk, R.t);
   R.r0 = __ldg(R.vert + sel4(id, R.f));
   R.r1 = __ldg(R.vert + sel4(id, (R.f + 1) & 3u));
@@ -151,24 +157,27 @@ __device__ __forceinline__ void begin_segment(const JobDev& J, Ray& R, uint32_t 
   R.lastZ = zp;
   R.cbi = (uint32_t)fmul(255.0f, sp);
   s_watch_saved[threadIdx.x] = 0xffffffffu;  // a new segment walks other states
+  return true;
 }
 
 // Composited mode: the pixel's next entry in its list, which stage (b)
 // wrote in descending (depth, face) order, skipping entries above the depth
 // where the previous segment left the mesh.  Returns false when the list is
-// done.
-__device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev& J,
-                                           Ray& R, bool first) {
-  (void)first;
+// done (or, checked build only, holds an id out of range: VFR_DEV_RANGE).
+__device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev& J, Ray& R,
+                                           uint32_t& status) {
   while (R.de < R.en) {
+    if (id_bad(R.ea + R.de, J.ent_cap)) break;
     const uint2 q = J.ent[R.ea + R.de];
     ++R.de;
     const float z = __uint_as_float(q.x);
     if (z > R.exitZ) continue;  // behind the ray already
+    if (id_bad(q.y, J.nExt)) break;
     const float4 p0 = J.planes[kPlaneStride * (size_t)q.y], p1 = J.planes[kPlaneStride * (size_t)q.y + 1];
-    begin_segment(J, R, q.y, z, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
+    if (!begin_segment(J, R, q.y, z, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y))) break;
     return true;
   }
+  if (kChecked && R.de < R.en) status |= kDevRange;
   return false;
 }
 
@@ -210,12 +219,12 @@ __device__ __forceinline__ uint32_t watched_step(const TraverseParams& P, Ray& R
 // RDELTA) / maxEdgeLength, the front's transfer-function entry, tau of the
 // front and of the back.  The step ends when sn is outside [0, 1] (:446).
 __device__ __forceinline__ void extinction(const SharedTables& S, const Ray& R, float zn, float sn,
-                                           uint32_t& st, uint32_t& tfi, float& taux,
+                                           bool& end, uint32_t& tfi, float& taux,
                                            float& tauy) {
   float dz = fsub(R.zp, zn);
   dz = dz < 0.0f ? -dz : dz;
   dz = below_rdelta(dz) ? 0.0f : dz;
-  st = (st == kContinue && ((sn < 0.0f) || (sn > 1.0f))) ? kSegmentEnd : st;
+  end = end || (sn < 0.0f) || (sn > 1.0f);
   // dz /= maxEdgeLength (:450): dz is 0 or at least 1e-12 and maxEdgeLength
   // below 2^80 (checked at upload; view set-up gives at most 2 sqrt 3), so
   // the quotient is never subnormal and div_by is exact
@@ -275,11 +284,11 @@ __device__ __forceinline__ StepColour composite(const TraverseParams& P, const S
 }
 
 // One iteration of the reference's while loop (:302-542).  The ways it can
-// end before compositing (a cycle or the step cap, no exit face, id range,
-// scalar or psi coordinate out of range) are folded into a status and the
-// arithmetic runs
-// on for every lane; the colour is only committed while the status says to
-// go on, so no lane takes an early branch.  The exact fallbacks of the
+// end before compositing (no exit face, scalar or psi coordinate out of
+// range; a cycle or the step cap in watched iterations; an id out of range
+// in the checked build) are folded into one flag and the arithmetic runs on
+// for every lane; the colour is only committed while the flag says to go
+// on, so no lane takes an early branch.  The exact fallbacks of the
 // plane, zeta and the psi coordinates are gathered into one rare block
 // after the fast path, so the step from the exit tests to the advance is
 // one straight run of code that the compiler schedules as a whole.
@@ -291,23 +300,29 @@ __device__ __forceinline__ StepColour composite(const TraverseParams& P, const S
 template <bool kWatched, bool kServe = false>
 __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTables& S, Ray& R) {
   ++R.iters;
-  uint32_t st = kContinue;
-  if (kWatched) st = watched_step(P, R);
+  const uint32_t wst = kWatched ? watched_step(P, R) : (uint32_t)kContinue;
+  bool end = wst != kContinue;
   const float e13x = fsub(R.r3.x, R.r1.x), e13y = fsub(R.r3.y, R.r1.y);
   const bool h1 = exit_test_v2(R.r1, R.r2, e13x, e13y, R.ox, R.oy);
   const bool h2 = exit_test(R.r2, R.r3, R.r0, R.ox, R.oy);
   const bool h3 = exit_test_v2(R.r3, R.r0, -e13x, -e13y, R.ox, R.oy);
   const uint32_t i = h1 ? 1u : (h2 ? 2u : (h3 ? 3u : 0u));
-  st = (st == kContinue && i == 0) ? kSegmentEnd : st;  // :353 no exit face
+  end = end || i == 0;  // :353 no exit face
   const uint32_t ex = (R.f + i) & 3u;
-  const uint32_t tn = sel4(R.w.n, ex);
-  const uint32_t q = sel4(R.w.q, ex);
+  const bool xo = (ex & 1u) != 0u, xh = (ex & 2u) != 0u;
+  const uint32_t tn = xh ? (xo ? R.w.n.w : R.w.n.z) : (xo ? R.w.n.y : R.w.n.x);
+  const uint32_t q = xh ? (xo ? R.w.q.w : R.w.q.z) : (xo ? R.w.q.y : R.w.q.x);
   const bool leaving = (tn == R.t);
-  st = (st == kContinue && tn >= R.nT) ? kRange : st;
-  // both loads of the step, issued before the plane solve that hides them
+  // both loads of the step, issued before the plane solve that hides them,
+  // whatever the exit: tn and the vertex word are valid ids for every face
+  // (a boundary face's record names the tet itself and vertex 0; the mesh's
+  // ids were validated at upload), so no branch cuts the step.  The checked
+  // build compares them first.
+  bool bad = id_bad(tn, R.nT) || id_bad(q & 0x07ffffffu, R.nV);
+  end = end || bad;
   WalkRec N = R.w;
   float4 nv = R.r0;
-  if (st == kContinue && !leaving) {
+  if (!bad) {
     N = ldg_walk(R.walk, tn);
     nv = __ldg(R.vert + (q & 0x07ffffffu));
   }
@@ -320,10 +335,10 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   Plane nf;
   const bool plane_ok = face_plane_fast(a, b, c, nf);
   float zn = plane_eval(R.ox, R.oy, nf.zx, nf.zy, nf.zz);
-  const uint32_t st0 = st;
+  const bool end0 = end;
   uint32_t tfi;
   float taux, tauy;
-  extinction(S, R, zn, plane_eval(R.ox, R.oy, nf.sx, nf.sy, nf.sz), st, tfi, taux, tauy);
+  extinction(S, R, zn, plane_eval(R.ox, R.oy, nf.sx, nf.sy, nf.sz), end, tfi, taux, tauy);
   bool z_ok, i_ok, j_ok;
   float zeta = zeta_fast(zeta_arg(taux, tauy), S.e2, z_ok);
   int ci = psi_coord_fast(taux, i_ok), cj = psi_coord_fast(tauy, j_ok);
@@ -331,28 +346,28 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
   // rare: the exact path for the lanes whose plane, zeta or psi coordinate
   // was not certified (a plane with a tiny coefficient; about one psi
   // coordinate in 2^10), before anything is committed
-  if ((!plane_ok && st0 == kContinue) || (st == kContinue && !(z_ok && i_ok && j_ok))) {
+  if ((!plane_ok && !end0) || (!end && !(z_ok && i_ok && j_ok))) {
     if (!plane_ok) {
       face_plane_ieee(a, b, c, nf);
       zn = plane_eval(R.ox, R.oy, nf.zx, nf.zy, nf.zz);
-      st = st0;
-      extinction(S, R, zn, plane_eval(R.ox, R.oy, nf.sx, nf.sy, nf.sz), st, tfi, taux, tauy);
+      end = end0;
+      extinction(S, R, zn, plane_eval(R.ox, R.oy, nf.sx, nf.sy, nf.sz), end, tfi, taux, tauy);
     }
     zeta = zeta_of(zeta_arg(taux, tauy), S.e2);
     ci = psi_coord(taux);
     cj = psi_coord(tauy);
     col = composite<false>(P, S, R, tfi, zeta, ci, cj);
   }
-  st = (st == kContinue && (ci | cj) < 0) ? kSegmentEnd : st;  // :468
-  if (st == kContinue) {
+  end = end || (ci | cj) < 0;  // :468
+  if (!end) {
     R.ar = col.r;
     R.ag = col.g;
     R.ab = col.b;
     R.tr = col.t;
     R.lastZ = zn;
     R.cbi = tfi;
-    st = leaving ? kSegmentEnd : st;  // :535
   }
+  const bool go_on = !end && !leaving;  // :535
   // advance to tn through its face fn: slots fn..fn+2 are the exit face's
   // vertices in tn's order (permutation code), slot fn+3 is the loaded
   // vertex.  Done whatever the status: once a ray's segment ends, nothing
@@ -374,19 +389,24 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
 #undef VFR_PICK
     R.r3 = nv;
   }
-  if (st == kContinue && code >= 6) {
+  if (go_on && code >= 6) {
     // shared face not matched by vertex ids: reload the tet's vertices
     const uint4 id = __ldg((kServe ? R.jp->tet : P.jobs[R.j].tet) + tn);
-    R.r0 = __ldg(R.vert + sel4(id, fn));
-    R.r1 = __ldg(R.vert + sel4(id, (fn + 1) & 3u));
-    R.r2 = __ldg(R.vert + sel4(id, (fn + 2) & 3u));
-    R.r3 = __ldg(R.vert + sel4(id, (fn + 3) & 3u));
+    bad = id_bad(id.x, R.nV) || id_bad(id.y, R.nV) || id_bad(id.z, R.nV) || id_bad(id.w, R.nV);
+    if (!bad) {
+      R.r0 = __ldg(R.vert + sel4(id, fn));
+      R.r1 = __ldg(R.vert + sel4(id, (fn + 1) & 3u));
+      R.r2 = __ldg(R.vert + sel4(id, (fn + 2) & 3u));
+      R.r3 = __ldg(R.vert + sel4(id, (fn + 3) & 3u));
+    }
   }
   R.w = N;
   R.t = tn;
   R.f = fn;
   R.zp = zn;
-  return st;
+  if (wst != kContinue) return wst;
+  if (bad) return kRange;
+  return go_on ? (uint32_t)kContinue : (uint32_t)kSegmentEnd;
 }
 
 // Start the ray of the job's local ray index `local`: its pixel, the
@@ -400,9 +420,14 @@ __device__ __forceinline__ bool start_ray(const TraverseParams& P, const JobDev&
   R.walk = J.walk;
   R.vert = J.vert;
   R.nT = J.nT;
+  R.nV = J.nV;
   R.watch = min(kWatchSteps, step_cap_of(P, J.nT));
   R.rmaxEdge = __drcp_rn((double)job_maxedge(J));
   R.p = J.rays[local];
+  if (id_bad(R.p, J.W * J.H)) {
+    status |= kDevRange;
+    return false;
+  }
   const uint32_t x = R.p % J.W, y = R.p / J.W;
   R.ox = obj_coord(x, J.W);
   R.oy = obj_coord(y, J.H);
@@ -412,17 +437,24 @@ __device__ __forceinline__ bool start_ray(const TraverseParams& P, const JobDev&
   const bool ref = kMode == 0 || (kMode == 2 && J.mode == 0);
   if (ref) {
     const uint32_t e = (uint32_t)J.winner[R.p];
+    if (id_bad(e, J.nExt)) {
+      status |= kDevRange;
+      return false;
+    }
     const float4 p0 = J.planes[kPlaneStride * (size_t)e];
     const float4 p1 = J.planes[kPlaneStride * (size_t)e + 1];
-    begin_segment(J, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
-                  plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y));
+    if (!begin_segment(J, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
+                       plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y))) {
+      status |= kDevRange;
+      return false;
+    }
     return true;
   }
   R.ea = J.ent_off[R.p];
   R.en = J.ent_cnt[R.p];
   R.exitZ = INFINITY;
   R.de = 0;
-  if (next_entry(P, J, R, true)) return true;
+  if (next_entry(P, J, R, status)) return true;
   finish_pixel(J, R);
   return false;
 }
@@ -510,7 +542,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) traverse_kernel(TraverseParam
     if (res == kSegmentEnd) {
       if (kMode == 1) {
         R.exitZ = R.lastZ;
-        if (next_entry(P, P.jobs[R.j], R, false)) continue;
+        if (next_entry(P, P.jobs[R.j], R, T.status)) continue;
       }
       finish_pixel(P.jobs[R.j], R);
     } else if (res == kCycle || res == kCap) {
@@ -702,7 +734,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) serve_kernel(ServeParams SP) 
       if (res == kSegmentEnd) {
         if (R.jp->mode == 1) {
           R.exitZ = R.lastZ;
-          fin = !next_entry(P, *R.jp, R, false);
+          fin = !next_entry(P, *R.jp, R, status);
         }
         if (fin) finish_pixel(*R.jp, R);
       } else if (res == kCycle || res == kCap) {
