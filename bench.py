@@ -10,9 +10,14 @@ Workloads (seeded synthetic meshes, transfer function and cameras):
   mixed    8 carved meshes with 16..128 cells per side and 256 jobs, each a
            random mesh, resolution in {128^2, 256^2, 512^2, 1024^2} and
            rotation; one step renders the 256 jobs.
-  served   resident carved meshes behind the request loop: Poisson arrivals at
-           several rates, requests of several resolutions; p50/p99 latency
-           and Mrays/s per rate.
+  served   32 resident carved meshes, N drawn uniformly from [16, 160] cells
+           per side (268 M tets in all), behind the request server: Poisson
+           arrivals at 50, 200, 1000 and 2000 requests/s, each request a
+           random mesh, resolution in {256^2, 512^2, 1024^2, 2048^2} and
+           rotation; p50/p99 latency, per-stage host timestamps and Mrays/s
+           per rate, against the same request mix rendered one request at a
+           time and as one batch.  Building the meshes on the host takes
+           about two minutes.
   convex24 one 512x512 view of the convex 24^3 mesh.
   large    one 2048x2048 view of the carved 256^3 mesh (100.7 M tets before
            carving, 85.6 M after: 4.1 GB of tet and walk records, far beyond
@@ -418,7 +423,8 @@ def cpu_baseline(wl, seconds):
     v, done, t = legs[nthreads]
     v1, done1, t1 = legs[1]
     return dict({"value": round(v, 4), "unit": "Mrays/s", "cores": nthreads, "kind": "reference",
-                 "sample": f"{done} of {len(wl['jobs'])} jobs, reference vfRayKernelCPU.cc "
+                 "sample": f"{done} job renders (the workload's {len(wl['jobs'])} jobs in order, "
+                           "cycling), reference vfRayKernelCPU.cc "
                            f"(-O3 -ffast-math) on {nthreads} threads (column strips), {t:.1f} s, "
                            "per job rotateVolume + normalizeVertices + buildLmt + the three stages",
                  "single_thread": {"value": round(v1, 4), "unit": "Mrays/s", "cores": 1,
@@ -818,6 +824,18 @@ def run_served(args):
                                 **{k: round(v, 3) for k, v in serve.percentiles(lat).items()},
                                 "mrays_s": round(rays / (span * 1e-3) / 1e6, 2),
                                 "mean_admitted_group": round(float(np.mean(list(groups.values()))), 1),
+                                # host timestamps per stage: queued (submit -> admitted), on the
+                                # device (admitted -> last ray seen done), copy-out (-> image in
+                                # the caller's buffer); medians and p99 in ms
+                                "stages_ms": {
+                                    k: {"p50": round(float(np.percentile(v, 50)), 3),
+                                        "p99": round(float(np.percentile(v, 99)), 3)}
+                                    for k, v in (
+                                        ("queued", [i["t_start_ms"] - i["t_submit_ms"] for i in infos]),
+                                        ("device", [i["t_ready_ms"] - i["t_start_ms"] for i in infos]),
+                                        ("copy_out", [i["t_done_ms"] - i["t_ready_ms"] for i in infos]))},
+                                "prep_ms_per_group": round((st1["prep_ms"] - st0["prep_ms"]) /
+                                                           max(1, st1["batches"] - st0["batches"]), 3),
                                 "drain_launches": st1["launches"] - st0["launches"]})
         stats = S.stats()
         done.set()

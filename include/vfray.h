@@ -267,6 +267,7 @@ typedef struct {
   uint32_t num_rays;
   uint64_t num_steps;
   uint32_t device_status;                      /* VFR_DEV_* bits of its job */
+  double t_ready_ms;   /* the worker saw its last ray finish, before the image copy */
 } vfr_request_info;
 
 typedef struct {

@@ -86,7 +86,7 @@ class RequestInfo(C.Structure):
     _fields_ = [("status", C.c_int), ("t_submit_ms", C.c_double), ("t_start_ms", C.c_double),
                 ("t_done_ms", C.c_double), ("batch_id", C.c_uint32), ("batch_jobs", C.c_uint32),
                 ("num_rays", C.c_uint32), ("num_steps", C.c_uint64),
-                ("device_status", C.c_uint32)]
+                ("device_status", C.c_uint32), ("t_ready_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -67,7 +67,7 @@ struct Req {
   uint64_t ticket = 0;
   vfr_request r{};
   uint64_t footprint = 0;
-  Clock::time_point t_submit, t_start, t_done;
+  Clock::time_point t_submit, t_start, t_ready, t_done;
   int status = VFR_OK;
   St state = St::Pending;
   bool claimed = false;  // a waiter holds it (a second waiter is refused)
@@ -399,6 +399,7 @@ bool vfr_server::poll_completions() {
           fail_all(VFR_ERR_CUDA);
           return true;
         }
+        q->t_ready = Clock::now();
         q->state = St::Copying;
         progress = true;
       }
@@ -693,6 +694,7 @@ int vfr_server_wait(vfr_server* s, uint64_t ticket, int timeout_ms, vfr_request_
     info->t_submit_ms = s->ms(q->t_submit);
     info->t_start_ms = q->t_start == Clock::time_point() ? info->t_submit_ms : s->ms(q->t_start);
     info->t_done_ms = s->ms(q->t_done);
+    info->t_ready_ms = q->t_ready == Clock::time_point() ? info->t_done_ms : s->ms(q->t_ready);
     info->batch_id = q->batch_id;
     info->batch_jobs = q->batch_jobs;
     info->num_rays = q->num_rays;
