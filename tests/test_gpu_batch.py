@@ -255,3 +255,46 @@ def test_mixed_workload_full_size_sampled_rays(renderer, oracle_lib):
     finally:
         for (_, mid, _, _) in cases:
             renderer.release_mesh(mid)
+
+
+def test_permuted_orbit_mesh_cycles_are_flagged(renderer, oracle_lib):
+    """The 64-view workload's carved 64^3 mesh with every tet listing its
+    vertices in a seeded random order: two of its ~10 M rays (views 9 and
+    45) walk in a cycle around a projected edge, where the reference's loop
+    never ends.  The batch stops exactly those two at the iteration where
+    the oracle's identical rule stops them (4,100), reports VFR_DEV_CYCLE,
+    and every other ray ends normally."""
+    vert, tet = synth.make_mesh(64, carved=True, view_seed=None, jitter_seed=0, scalar_seed=1,
+                                carve_seed=4)
+    p = vb.prepare(vert, synth.permute_tet_vertices(tet, 0))
+    tf = synth.transfer_function(2)
+    psi = vb.psi_table()
+    views = synth.orbit_views(64, seed=3)
+    W = H = 512
+    renderer.upload_tables(tf, psi)
+    mid = renderer.upload_mesh(p["vert"], p["tet"], p["con"], p["extf"], p["lmt"])
+    try:
+        B = vbatch.BatchRenderer(renderer, [(mid, mv, W, H) for mv in views])
+        try:
+            B.prepare()
+            B.run()
+            with pytest.raises(vb.VfrError, match="cycle=32"):
+                B.stats()
+            steps = np.empty(len(views) * W * H, np.uint32)
+            B.read(steps=steps)
+        finally:
+            B.close()
+        steps = steps.reshape(len(views), W * H)
+        long_ = np.argwhere(steps > 4095)
+        assert [tuple(x) for x in long_.tolist()] == [(9, 162545), (45, 153268)]
+        assert np.all(steps[steps > 4095] == 4100)
+        for j, pix in long_.tolist():
+            vv = vb.normalize(vb.rotate(p["vert"], views[j]))
+            m = oracle_lib.mesh(vv, p["tet"], p["con"], p["extf"], tf, psi,
+                                vb.build_lmt(vv, p["tet"])[0])
+            wr = oracle_lib.winners(m, W, H).ravel()
+            t = oracle_lib.trace_pixels(m, W, H, np.array([pix], np.uint32),
+                                        np.array([wr[pix]], np.uint32))
+            assert int(t["steps"][0]) == int(steps[j, pix]) == 4100
+    finally:
+        renderer.release_mesh(mid)

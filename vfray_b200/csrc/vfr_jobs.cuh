@@ -553,12 +553,29 @@ __global__ void __launch_bounds__(256) tile_kernel(const JobDev* __restrict__ jo
       __syncthreads();
       return min(256u, b1 - c);
     };
-    // pass 1: entries per pixel
+    // pass 1: entries per pixel.  A tile whose bin fits one staged chunk
+    // (the common case) also keeps which of the chunk's faces cover each
+    // pixel, as a 256-bit mask in registers, so that pass 2 neither stages
+    // nor tests the faces again.
+    const bool one_chunk = b1 - b0 <= 256u;
+    uint32_t cov[8];
     uint32_t count = 0;
     for (uint32_t c = b0; c < b1; c += 256) {
-      const uint32_t m = stage(c);
-      if (live)
-        for (uint32_t k = 0; k < m; ++k) count += covers(F[k]) ? 1u : 0u;
+      const uint32_t staged = stage(c);  // every thread: stage() synchronises the block
+      const uint32_t m = live ? staged : 0u;
+#pragma unroll
+      for (uint32_t w = 0; w < 8; ++w) {  // w is a constant after unrolling: cov stays in registers
+        uint32_t bits = 0;
+        const uint32_t kn = min(m, 32u * w + 32u);
+        for (uint32_t k = 32u * w; k < kn; ++k)
+          if (covers(F[k])) bits |= 1u << (k & 31u);
+        cov[w] = bits;
+        count += __popc(bits);
+      }
+    }
+    if (b1 == b0) {
+#pragma unroll
+      for (uint32_t w = 0; w < 8; ++w) cov[w] = 0;
     }
     // block scan of the counts
     uint32_t x = count;
@@ -594,23 +611,32 @@ __global__ void __launch_bounds__(256) tile_kernel(const JobDev* __restrict__ jo
     }
     // pass 2: each pixel's entries, inserted in descending (depth, face) order
     uint32_t n = 0;
-    for (uint32_t c = b0; c < b1; c += 256) {
-      const uint32_t m = stage(c);
-      if (live && fits && count)
-        for (uint32_t k = 0; k < m; ++k) {
-          const TileFace& f = F[k];
-          if (!covers(f)) continue;
-          const float z = plane_eval(ox, oy, f.zx, f.zy, f.zz);
-          uint32_t q = n++;
-          while (q > 0) {
-            const uint2 a = ent[off + q - 1];
-            const float za = __uint_as_float(a.x);
-            if (za > z || (za == z && a.y > f.e)) break;
-            ent[off + q] = a;
-            --q;
-          }
-          ent[off + q] = make_uint2(__float_as_uint(z), f.e);
-        }
+    auto insert = [&](const TileFace& f) {
+      const float z = plane_eval(ox, oy, f.zx, f.zy, f.zz);
+      uint32_t q = n++;
+      while (q > 0) {
+        const uint2 a = ent[off + q - 1];
+        const float za = __uint_as_float(a.x);
+        if (za > z || (za == z && a.y > f.e)) break;
+        ent[off + q] = a;
+        --q;
+      }
+      ent[off + q] = make_uint2(__float_as_uint(z), f.e);
+    };
+    if (one_chunk) {  // F still holds the chunk pass 1 staged
+      if (live && fits && count) {
+#pragma unroll
+        for (uint32_t w = 0; w < 8; ++w)
+          for (uint32_t bits = cov[w]; bits; bits &= bits - 1u)
+            insert(F[32u * w + (uint32_t)(__ffs(bits) - 1)]);
+      }
+    } else {
+      for (uint32_t c = b0; c < b1; c += 256) {
+        const uint32_t m = stage(c);
+        if (live && fits && count)
+          for (uint32_t k = 0; k < m; ++k)
+            if (covers(F[k])) insert(F[k]);
+      }
     }
   }
 }
