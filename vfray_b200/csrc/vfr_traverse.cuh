@@ -166,18 +166,26 @@ __device__ __forceinline__ bool begin_segment(const JobDev& J, Ray& R, uint32_t 
 // done (or, checked build only, holds an id out of range: VFR_DEV_RANGE).
 __device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev& J, Ray& R,
                                            uint32_t& status) {
+  bool bad = false;
   while (R.de < R.en) {
-    if (id_bad(R.ea + R.de, J.ent_cap)) break;
+    if (id_bad(R.ea + R.de, J.ent_cap)) {
+      bad = true;
+      break;
+    }
     const uint2 q = J.ent[R.ea + R.de];
     ++R.de;
     const float z = __uint_as_float(q.x);
     if (z > R.exitZ) continue;  // behind the ray already
-    if (id_bad(q.y, J.nExt)) break;
+    if (id_bad(q.y, J.nExt)) {
+      bad = true;
+      break;
+    }
     const float4 p0 = J.planes[kPlaneStride * (size_t)q.y], p1 = J.planes[kPlaneStride * (size_t)q.y + 1];
-    if (!begin_segment(J, R, q.y, z, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y))) break;
-    return true;
+    if (begin_segment(J, R, q.y, z, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y))) return true;
+    bad = true;
+    break;
   }
-  if (kChecked && R.de < R.en) status |= kDevRange;
+  if (bad) status |= kDevRange;
   return false;
 }
 
