@@ -197,15 +197,21 @@ VFR_API void vfr_batch_destroy(vfr_batch* b);
 VFR_API int vfr_batch_set_jobs(vfr_batch* b, const vfr_job* jobs, uint32_t n, int mode);
 /* Captures the whole chain as a CUDA graph; vfr_batch_run then replays it. */
 VFR_API int vfr_batch_capture(vfr_batch* b);
-/* Enqueues the batch on the context stream (asynchronous). */
+/* Enqueues the batch on its stream (asynchronous): the context stream, or
+ * the one vfr_batch_set_stream gave it. */
 VFR_API int vfr_batch_run(vfr_batch* b);
+/* Gives the batch a stream of its own (a cudaStream_t of the context's
+ * device; NULL: the context stream again) for its runs, camera uploads,
+ * reads and stats.  Two batches on two streams overlap: one's copies run
+ * beside the other's kernels. */
+VFR_API int vfr_batch_set_stream(vfr_batch* b, void* stream);
 /* Waits, then fills per-job stats (n entries at most); returns the status. */
 VFR_API int vfr_batch_stats(vfr_batch* b, vfr_render_stats* per_job, uint32_t n);
 /* Device output pointers of a job (the batch's own when it owns them). */
 VFR_API int vfr_batch_output(vfr_batch* b, uint32_t job, uint8_t** rgb8_dev, float** rgba_dev,
                              uint32_t** steps_dev);
 /* Replaces the model-view of every job (n = the batch's job count): one
- * asynchronous host-to-device copy on the context stream of the first three
+ * asynchronous host-to-device copy on the batch's stream of the first three
  * rows of each matrix, after which the next vfr_batch_run -- a replayed
  * graph included -- renders with the new cameras.  mv16: n row-major 4x4
  * matrices in host memory (pinned memory gives a full-speed copy), left
@@ -218,6 +224,14 @@ VFR_API int vfr_batch_set_cameras(vfr_batch* b, const float* mv16, uint32_t n);
  * one copy per kind. */
 VFR_API int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host,
                            uint32_t* steps_host);
+/* The same copies, enqueued on the batch's stream without waiting: the host
+ * buffers (pinned memory, for the copies to be asynchronous) hold the
+ * outputs once the stream has run them (vfr_batch_synchronize); the next
+ * vfr_batch_run of this batch is ordered after them. */
+VFR_API int vfr_batch_read_async(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host,
+                                 uint32_t* steps_host);
+/* Waits for everything enqueued on the batch's stream. */
+VFR_API int vfr_batch_synchronize(vfr_batch* b);
 /* Autotuner: times stages (b) and (c) of the batch over a grid of the
  * knobs above (traversal register budget, refill threshold, traversal CTAs
  * per SM, ray-tile shape, stage (b) warps per SM), best of `reps` runs each,

@@ -160,6 +160,52 @@ def test_cameras_change_between_host_runs(renderer, scene):
         B.close()
 
 
+def test_two_batches_on_two_streams_take_turns(renderer, scene):
+    """A frame loop over two batches of the same jobs, each on a stream of
+    its own: per step, cameras in, run, an asynchronous read into that
+    batch's pinned buffer.  After both streams are done, each step's images
+    equal the same cameras rendered by one batch with a waiting read."""
+    import torch
+
+    jobs = [j for j in scene if j[1] is not None]
+    npx = sum(W * H for (_, _, W, H) in jobs)
+    pair = [vbatch.BatchRenderer(renderer, jobs), vbatch.BatchRenderer(renderer, jobs)]
+    ref = vbatch.BatchRenderer(renderer, jobs)
+    try:
+        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+        for x, s in zip(pair, streams):
+            x.prepare()
+            x.set_stream(s)
+        ref.prepare()
+        steps = [synth.orbit_views(len(jobs), seed=31 + k) for k in range(4)]
+        cams = [torch.empty((len(jobs), 4, 4), dtype=torch.float32, pin_memory=True)
+                for _ in steps]
+        outs = [torch.empty(npx * 3, dtype=torch.uint8, pin_memory=True) for _ in steps]
+        got = []
+        for k, views in enumerate(steps):
+            x = pair[k & 1]
+            if k >= 2:  # this batch's previous step is read back: keep it
+                x.synchronize()
+                got.append(outs[k - 2].numpy().copy())
+            cams[k].copy_(torch.from_numpy(views))
+            x.set_cameras(cams[k])
+            x.run()
+            x.read_async(rgb8=outs[k])
+        for x in pair:
+            x.synchronize()
+        got += [outs[2].numpy().copy(), outs[3].numpy().copy()]
+        want = torch.empty(npx * 3, dtype=torch.uint8, pin_memory=True)
+        for k, views in enumerate(steps):
+            ref.run_host(want, cameras=torch.from_numpy(views).contiguous())
+            assert np.array_equal(got[k], want.numpy()), k
+        assert not np.array_equal(got[0], got[1])
+        for x in pair:
+            x.stats()
+    finally:
+        for x in pair + [ref]:
+            x.close()
+
+
 def test_cycling_ray_is_stopped(renderer, oracle_lib):
     """A mesh whose tets list their vertices in random order, seen from a
     view where one ray's walk cycles among the tets around an edge (the

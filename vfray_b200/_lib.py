@@ -138,6 +138,9 @@ SIGNATURES = {
     "vfr_batch_stats": (_i, [_vp, C.POINTER(RenderStats), _u32]),
     "vfr_batch_output": (_i, [_vp, _u32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
     "vfr_batch_read": (_i, [_vp, _vp, _vp, _vp]),
+    "vfr_batch_read_async": (_i, [_vp, _vp, _vp, _vp]),
+    "vfr_batch_synchronize": (_i, [_vp]),
+    "vfr_batch_set_stream": (_i, [_vp, _vp]),
     "vfr_batch_set_cameras": (_i, [_vp, _vp, _u32]),
     "vfr_batch_autotune": (_i, [_vp, _i, C.POINTER(Tuning)]),
     "vfr_batch_scratch_bytes": (_i, [_vp, C.POINTER(C.c_uint64)]),

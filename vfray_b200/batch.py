@@ -101,14 +101,33 @@ class BatchRenderer:
 
     def launches_per_run(self) -> int:
         # init, rotate, normalize, maxedge, visible, compact, prefix, raster,
-        # raylist, prefix, traverse (composited: + 2 raster passes, 2 scans, totals)
-        return 11 if self.mode == _lib.MODE_REF else 16
+        # raylist, prefix, traverse (composited: the raster replaced by two
+        # bin passes, a two-kernel scan and the tile kernel)
+        return 11 if self.mode == _lib.MODE_REF else 15
 
     def read(self, rgb8=None, rgba=None, steps=None):
         """Copy every job's outputs (concatenated in job order) into host
         buffers (numpy arrays or pinned torch tensors) and wait."""
         check(self.lib.vfr_batch_read(self.h, ptr(rgb8), ptr(rgba), ptr(steps)), self.r.h,
               "vfr_batch_read")
+
+    def read_async(self, rgb8=None, rgba=None, steps=None):
+        """The same copies, enqueued on the batch's stream without waiting
+        (pinned host buffers; they hold the outputs after synchronize())."""
+        check(self.lib.vfr_batch_read_async(self.h, ptr(rgb8), ptr(rgba), ptr(steps)), self.r.h,
+              "vfr_batch_read_async")
+
+    def synchronize(self):
+        """Wait for everything enqueued on the batch's stream."""
+        check(self.lib.vfr_batch_synchronize(self.h), self.r.h, "vfr_batch_synchronize")
+
+    def set_stream(self, stream):
+        """Run this batch on its own stream (a torch.cuda.Stream or a raw
+        cudaStream_t handle; None: the renderer's stream again)."""
+        handle = getattr(stream, "cuda_stream", stream)
+        self._stream = stream  # alive while the batch uses it
+        check(self.lib.vfr_batch_set_stream(self.h, C.c_void_p(handle) if handle else None),
+              self.r.h, "vfr_batch_set_stream")
 
     def set_cameras(self, mv):
         """New model-views for every job, (njobs, 4, 4) row-major float32 in

@@ -1239,8 +1239,10 @@ int vfr_batch_set_cameras(vfr_batch* b, const float* mv16, uint32_t n) {
                 "camera upload");
 }
 
-int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host, uint32_t* steps_host) {
-  vfr::Range nvtx("vfr_batch_read");
+// The batch's outputs into host buffers: enqueued on the batch's stream,
+// then (wait) a synchronisation of that stream.
+static int batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host, uint32_t* steps_host,
+               bool wait) {
   if (!b || !b->b.njobs) return VFR_ERR_STATE;
   if (!b->owner) return VFR_ERR_STATE;
   Ctx& C = b->owner->impl;
@@ -1281,8 +1283,32 @@ int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host, uint32_t*
   if (!rc)
     rc = read((char*)steps_host, sizeof(uint32_t),
               [](const JobSpec& q) { return (const void*)q.steps; }, "steps read");
-  if (!rc) rc = C.cuda(cudaStreamSynchronize(b->b.st()), "batch read");
+  if (!rc && wait) rc = C.cuda(cudaStreamSynchronize(b->b.st()), "batch read");
   return rc;
+}
+
+int vfr_batch_read(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host, uint32_t* steps_host) {
+  vfr::Range nvtx("vfr_batch_read");
+  return batch_read(b, rgb8_host, rgba_host, steps_host, true);
+}
+
+int vfr_batch_read_async(vfr_batch* b, uint8_t* rgb8_host, float* rgba_host,
+                         uint32_t* steps_host) {
+  vfr::Range nvtx("vfr_batch_read_async");
+  return batch_read(b, rgb8_host, rgba_host, steps_host, false);
+}
+
+int vfr_batch_synchronize(vfr_batch* b) {
+  if (!b || !b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  return C.cuda(cudaStreamSynchronize(b->b.st()), "batch synchronize");
+}
+
+int vfr_batch_set_stream(vfr_batch* b, void* stream) {
+  if (!b || !b->owner) return VFR_ERR_STATE;
+  b->b.stream = static_cast<cudaStream_t>(stream);
+  return VFR_OK;
 }
 
 int vfr_batch_scratch_bytes(vfr_batch* b, uint64_t* bytes) {
