@@ -685,7 +685,12 @@ def run_ours(args, rank, world, dist):
                 "launch_ms_mean": round(float(trav_ms.mean()), 4),
                 "gsteps_per_s": round(float(steps_step / launches_per_trav * len(trav_ms)
                                             / (trav_ms.sum() * 1e-3) / 1e9), 2),
-                "stage_ms_mean": [round(float(x), 4) for x in prof.mean(0)]}
+                "stage_ms_mean": [round(float(x), 4) for x in prof.mean(0)],
+                # the same launch counted without the walk's vertex reuse: the
+                # record and all 4 vertices of every tet (32 + 4 x 16 B)
+                "no_reuse": {"bytes_per_step": 96,
+                             "achieved": round(float(achieved * 96 / BYTES_PER_STEP), 1),
+                             "frac": round(float(achieved * 96 / BYTES_PER_STEP / peak), 4)}}
     runner.close()
     for m in mids:
         r.release_mesh(m)
