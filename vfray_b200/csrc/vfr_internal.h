@@ -185,7 +185,7 @@ struct Ctx {
   std::vector<void*> batches;  // live vfr_batch handles, detached when the context goes
 
   ~Ctx();
-  void prof_mark(int k);
+  void prof_mark(int k, cudaStream_t on = nullptr);  // on: the stream the stages run on (null: the context stream)
   int fail(int code, const std::string& msg);
   int cuda(cudaError_t e, const char* what);
   int grow(Buf& b, size_t bytes, const char* what);

@@ -95,7 +95,7 @@ Mesh* Ctx::mesh(int id) {
   return meshes[id].get();
 }
 
-void Ctx::prof_mark(int k) {
+void Ctx::prof_mark(int k, cudaStream_t on) {
   if (!profile) return;
   if (k == 0) {
     StageEvents s;
@@ -107,7 +107,7 @@ void Ctx::prof_mark(int k) {
     }
     prof_live.push_back(s);
   }
-  cudaEventRecord(prof_live.back().e[k], stream);
+  cudaEventRecord(prof_live.back().e[k], on ? on : stream);
 }
 
 const void* Ctx::traverse_fn(int mode, uint32_t variant) {
@@ -590,6 +590,14 @@ struct vfr_batch {
   Batch b;
 };
 
+// Waits for the context stream and for the streams of the context's batches
+// (a batch may run on a stream of its own): done before memory that their
+// launches may read is freed or overwritten.
+static void sync_context(Ctx& C) {
+  cudaStreamSynchronize(C.stream);
+  for (void* p : C.batches) cudaStreamSynchronize(static_cast<vfr_batch*>(p)->b.st());
+}
+
 #define CTX_OR_FAIL(c)              \
   if (!(c)) return VFR_ERR_INVALID; \
   Ctx& C = (c)->impl;               \
@@ -674,7 +682,7 @@ int vfr_create(vfr_ctx** out, int device) {
 void vfr_destroy(vfr_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->impl.device);
-  cudaStreamSynchronize(c->impl.stream);
+  sync_context(c->impl);
   // batches that outlive their context keep only their own memory; any call
   // on them but vfr_batch_destroy then returns VFR_ERR_STATE
   for (void* p : c->impl.batches) {
@@ -766,7 +774,7 @@ int vfr_tables_upload(vfr_ctx* c, const float* tf, const float* psi) {
     if (!rc) rc = C.cuda(cudaMalloc(&C.d_psi, sizeof(float) * 512 * 512), "psi alloc");
     if (rc) return rc;
   }
-  cudaStreamSynchronize(C.stream);
+  sync_context(C);
   double e2[64];
   for (int j = 0; j < 64; ++j) e2[j] = (double)std::exp2l((long double)j / 64.0L);
   int rc = C.cuda(cudaMemcpy(C.d_tf, tf, sizeof(float) * 1024, cudaMemcpyHostToDevice), "tf upload");
@@ -836,7 +844,7 @@ int vfr_mesh_upload(vfr_ctx* c, const float* vert4, uint32_t nV, const uint32_t*
 int vfr_mesh_release(vfr_ctx* c, int id) {
   CTX_OR_FAIL(c);
   if (!C.mesh(id)) return C.fail(VFR_ERR_STATE, "unknown mesh id");
-  cudaStreamSynchronize(C.stream);
+  sync_context(C);
   if (C.plain.njobs && C.plain.specs[0].mesh == id) {
     C.plain.njobs = 0;
     C.stage = 0;
@@ -1037,6 +1045,7 @@ void vfr_batch_destroy(vfr_batch* b) {
     Ctx& C = b->owner->impl;
     cudaSetDevice(C.device);
     cudaStreamSynchronize(C.stream);
+    cudaStreamSynchronize(b->b.st());
     C.batches.erase(std::remove(C.batches.begin(), C.batches.end(), (void*)b), C.batches.end());
   }
   delete b;
@@ -1065,6 +1074,7 @@ int vfr_batch_set_jobs(vfr_batch* b, const vfr_job* jobs, uint32_t n, int mode) 
     own = own || (!jobs[j].rgb8_dev && !jobs[j].rgba_dev && !jobs[j].steps_dev);
   }
   cudaStreamSynchronize(C.stream);
+  cudaStreamSynchronize(b->b.st());  // its own stream's runs read the arenas the layout may grow
   int rc = b->b.layout(s, mode, own);
   if (!rc) rc = b->b.upload(false);
   return rc;
@@ -1088,20 +1098,20 @@ int vfr_batch_run(vfr_batch* b) {
   cudaSetDevice(C.device);
   if (!C.d_tf) return C.fail(VFR_ERR_STATE, "tables not uploaded");
   if (C.profile && !b->b.exec) {  // per-stage events need the direct launches
-    C.prof_mark(0);
+    C.prof_mark(0, b->b.st());
     int rc = b->b.enqueue_a();
-    C.prof_mark(1);
+    C.prof_mark(1, b->b.st());
     if (!rc) rc = b->b.enqueue_b();
-    C.prof_mark(2);
+    C.prof_mark(2, b->b.st());
     if (!rc) rc = b->b.enqueue_c();
-    C.prof_mark(3);
+    C.prof_mark(3, b->b.st());
     return rc;
   }
-  C.prof_mark(0);
-  C.prof_mark(1);
-  C.prof_mark(2);
+  C.prof_mark(0, b->b.st());
+  C.prof_mark(1, b->b.st());
+  C.prof_mark(2, b->b.st());
   int rc = b->b.run();
-  C.prof_mark(3);
+  C.prof_mark(3, b->b.st());
   return rc;
 }
 
@@ -1181,11 +1191,11 @@ int vfr_batch_autotune(vfr_batch* b, int reps, vfr_tuning* out) {
             float ms = 1e30f;
             for (int r = 0; r < reps + 1 && !rc; ++r) {
               rc = b->b.enqueue_a();
-              cudaEventRecord(e0, C.stream);
+              cudaEventRecord(e0, b->b.st());
               if (!rc) rc = b->b.enqueue_b();
-              cudaEventRecord(e1, C.stream);
+              cudaEventRecord(e1, b->b.st());
               if (!rc) rc = b->b.enqueue_c();
-              cudaEventRecord(e2, C.stream);
+              cudaEventRecord(e2, b->b.st());
               if (!rc) rc = C.cuda(cudaEventSynchronize(e2), "autotune");
               float m = 0;
               cudaEventElapsedTime(&m, e0, e2);
