@@ -34,7 +34,11 @@ metric through the host-buffer API: every step copies the step's cameras from
 pinned host memory to the device and the RGB8 images back to pinned host
 memory, inside the timed region, as a frame loop does it: two batches of the
 same jobs on two streams take turns, so one step's image copy overlaps the
-next step's kernels, and the clock stops when both streams are done.  ``roofline`` divides the traversal kernel's
+next step's kernels, and the clock stops when both streams are done.
+``served_same_jobs`` submits the step's jobs as requests to the request
+server (three rounds at once, after an untimed one): the served form at
+saturation on the same work, with p50/p99 latency, against the plain
+per-view call (``plain_per_view``).  ``roofline`` divides the traversal kernel's
 algorithmic bytes (48 B per tet-walk step: one 32-byte walk record + one new
 16-byte vertex) by its event-timed launch duration.  ``cpu_baseline`` times
 the reference's own CPU kernels (built from the reference sources into
@@ -515,6 +519,36 @@ def setup_gpu(wl, dev):
     return r, stream, mids
 
 
+def served_leg(r, jobs, mode, rounds=3):
+    """The step's jobs as requests to the request server (the served form):
+    one untimed round, then `rounds` rounds submitted at once, so the server
+    runs at saturation on this workload.  Latency is submit to image in the
+    caller's host buffer.  Per GPU (each rank measures its own)."""
+    from vfray_b200 import serve
+
+    with serve.Server(r, budget_bytes=64 << 30) as S:
+        def submit_all(n):
+            return [S.submit(mid, W, H, mv=mv, mode=mode)
+                    for _ in range(n) for (mid, mv, W, H) in jobs]
+        for t in submit_all(1):
+            S.wait(t, timeout_ms=600000)
+        st0 = S.stats()
+        t0 = time.perf_counter()
+        infos = [S.wait(t, timeout_ms=600000)[1] for t in submit_all(rounds)]
+        dt = time.perf_counter() - t0
+        st1 = S.stats()
+    assert all(i["status"] == 0 for i in infos)
+    lat = [i["t_done_ms"] - i["t_submit_ms"] for i in infos]
+    pc = serve.percentiles(lat)
+    return {"value": round(sum(i["num_rays"] for i in infos) / dt / 1e6, 2), "unit": "Mrays/s",
+            "requests": len(infos), "p50_ms": round(pc["p50"], 3), "p99_ms": round(pc["p99"], 3),
+            "drain_launches": st1["launches"] - st0["launches"],
+            "admitted_groups": st1["batches"] - st0["batches"],
+            "how": (f"the step's {len(jobs)} jobs submitted {rounds} times at once to the request "
+                    "server (one persistent drain launch; images into host memory), after one "
+                    "untimed round")}
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -654,6 +688,7 @@ def run_ours(args, rank, world, dist):
     if runner2 is not None:
         runner.set_stream(None)
         runner2.close()
+    served = served_leg(r, jobs, mode) if args.form == "batched" else None
 
     times = max_over_ranks([t_main, t_e2e, t_plain, t_batch], dist, dev)
     t_main, t_e2e, t_plain, t_batch = times
@@ -713,6 +748,8 @@ def run_ours(args, rank, world, dist):
         "plain_per_view": {"value": round(float(mrays(t_plain, kp)), 2), "unit": "Mrays/s",
                            "ms_per_step": round(float(t_plain / kp), 3)},
         "batched_over_plain": round(float(t_plain / t_batch), 3),
+        "served_same_jobs": (dict(served, over_plain=round(float(served["value"] / mrays(t_plain, kp)), 3))
+                             if served else None),
         "e2e": {"value": round(float(e2e), 2), "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(npix * 3), "ms_per_step": round(float(t_e2e / K), 3),
                 "copies": ("per step: one 2D copy of the jobs' cameras (host to device), the "
