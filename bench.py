@@ -835,6 +835,11 @@ def run_served(args):
     # the same mix, plain (one request at a time, host buffers) and batched
     mix = served_requests(64, nm, np.random.default_rng(99))
     outs = [np.empty((s, s, 3), np.uint8) for (_, _, s) in mix]
+    # warm-up, untimed: every mesh once (its distinct edges, which a view
+    # with a model-view needs, are built on first use; the server builds
+    # them at start), then the first requests of the mix
+    for m in range(nm):
+        r.render_into_host(mids[m], 64, 64, np.empty((64, 64, 3), np.uint8), mv=mix[0][1])
     for k, (m, mv, s) in enumerate(mix[:4]):
         r.render_into_host(mids[m], s, s, outs[k], mv=mv)
     t0 = time.perf_counter()
