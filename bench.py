@@ -245,14 +245,23 @@ class Clocks:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.index), "-lms", "200"],
+                                          "-i", str(self.index), "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # the timed region starts once the sampler runs (its start-up takes
+        # longer than a short timed region)
+        t_end = time.time() + 3.0
+        while self.proc and time.time() < t_end and self.proc.poll() is None:
+            self.f.flush()
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *exc):
         if self.proc:
+            time.sleep(0.06)  # one more sample at the end of the region
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
