@@ -202,8 +202,9 @@ VFR_API int vfr_batch_capture(vfr_batch* b);
 VFR_API int vfr_batch_run(vfr_batch* b);
 /* Gives the batch a stream of its own (a cudaStream_t of the context's
  * device; NULL: the context stream again) for its runs, camera uploads,
- * reads and stats.  Two batches on two streams overlap: one's copies run
- * beside the other's kernels. */
+ * reads and stats; waits first for what the batch's previous stream still
+ * holds.  Two batches on two streams overlap: one's copies run beside the
+ * other's kernels. */
 VFR_API int vfr_batch_set_stream(vfr_batch* b, void* stream);
 /* Waits, then fills per-job stats (n entries at most); returns the status. */
 VFR_API int vfr_batch_stats(vfr_batch* b, vfr_render_stats* per_job, uint32_t n);

@@ -1317,6 +1317,10 @@ int vfr_batch_synchronize(vfr_batch* b) {
 
 int vfr_batch_set_stream(vfr_batch* b, void* stream) {
   if (!b || !b->owner) return VFR_ERR_STATE;
+  Ctx& C = b->owner->impl;
+  cudaSetDevice(C.device);
+  // work already enqueued on the old stream is not ordered with the new one
+  if (int rc = C.cuda(cudaStreamSynchronize(b->b.st()), "batch stream switch")) return rc;
   b->b.stream = static_cast<cudaStream_t>(stream);
   return VFR_OK;
 }
