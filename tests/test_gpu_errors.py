@@ -51,6 +51,27 @@ def test_rejects_interior_face_in_ext_list(renderer, case):
            case["lmt"])
 
 
+def test_rejects_empty_mesh_and_empty_batch(renderer, case):
+    """A mesh without vertices or tets is refused at upload; a batch without
+    jobs is refused when its jobs are set; the context stays usable."""
+    v0 = np.zeros((0, 4), np.float32)
+    t0 = np.zeros((0, 4), np.uint32)
+    e0 = np.zeros((0, 2), np.uint32)
+    expect(vb._lib.VFR_ERR_INVALID, renderer.upload_mesh, v0, case["tet"], case["con"],
+           case["extf"], case["lmt"])
+    expect(vb._lib.VFR_ERR_INVALID, renderer.upload_mesh, case["vert"], t0, t0, e0, case["lmt"])
+    from vfray_b200 import batch as vbatch
+
+    with pytest.raises(vb.VfrError) as e:
+        vbatch.BatchRenderer(renderer, [])
+    assert e.value.status == vb._lib.VFR_ERR_INVALID
+    mid = renderer.upload_mesh(case["vert"], case["tet"], case["con"], case["extf"], case["lmt"])
+    try:
+        renderer.render(mid, 16, 16)
+    finally:
+        renderer.release_mesh(mid)
+
+
 def test_rejects_unusable_max_edge(renderer, case):
     """maxEdgeLength enters the traversal through a reciprocal whose quotients
     must stay normal: values from 2^80 up, and NaN, are refused."""
