@@ -682,7 +682,8 @@ __global__ void __launch_bounds__(256) tile_kernel(const JobDev* __restrict__ jo
   }
 }
 
-// Ray lists: the pixels with an entry face, in screen tiles of 32 pixels
+// Ray lists: the pixels with an entry face, as start records (RayStart),
+// in screen tiles of 32 pixels
 // (tw x 32/tw, one warp per tile, tiles of all jobs in one index space) so
 // that neighbouring rays, which walk neighbouring tets, are neighbours in the
 // list and share warps.  Pixels without one are cleared in the outputs here
@@ -701,17 +702,44 @@ __global__ void __launch_bounds__(256) raylist_kernel(const JobDev* __restrict__
   const uint32_t x = (tile % tx) * tw + (lane % tw), y = (tile / tx) * th + (lane / tw);
   bool has = false;
   uint32_t p = 0;
+  RayStart rs = {0u, 0u, 0u, 0u};
   const bool inside = x < J.W && y < J.H;
   if (inside) {
     p = y * J.W + x;
-    has = mode == 0 ? (J.winner[p] >= 0) : (J.ent_cnt[p] > 0);
+    rs.p = p;
+    if (mode == 0) {
+      // the winning face's segment start, computed as the traversal would
+      // (vfRayKernelCPU.cc:250-279): object coordinates of the pixel, the
+      // plane's depth and scalar there, the face's tet and entry face
+      const int32_t w = J.winner[p];
+      has = w >= 0;
+      if (has && id_bad((uint32_t)w, J.nExt)) {
+        atomicOr(&J.ctr->status, kDevRange);
+        has = false;
+      }
+      if (has) {
+        const float4* pl = J.planes + kPlaneStride * (size_t)w;
+        const float4 p0 = pl[0], p1 = pl[1];
+        const float ox = obj_coord(x, J.W), oy = obj_coord(y, J.H);
+        const uint2 tf = J.extf[w];
+        rs.tf = (tf.x << 2) | (tf.y & 3u);
+        rs.zp = __float_as_uint(plane_eval(ox, oy, p0.x, p0.y, p0.z));
+        rs.cbi = (uint32_t)fmul(255.0f, plane_eval(ox, oy, p0.w, p1.x, p1.y));
+        if (id_bad(tf.x, J.nT)) {
+          atomicOr(&J.ctr->status, kDevRange);
+          has = false;
+        }
+      }
+    } else {
+      has = J.ent_cnt[p] > 0;
+    }
   }
   const uint32_t m = __ballot_sync(0xffffffffu, has);
   if (m) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&J.ctr->nrays, (uint32_t)__popc(m));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (has) J.rays[base + __popc(m & ((1u << lane) - 1u))] = p;
+    if (has) J.rays[base + __popc(m & ((1u << lane) - 1u))] = rs;
   }
   if (inside && !has) {
     if (J.rgb8) {

@@ -238,7 +238,7 @@ size_t Batch::arena_bytes(Ctx& C, const std::vector<JobSpec>& s, int mode, uint3
              a(sizeof(uint32_t) * (2 * (nj + 1) + 4)) + a(sizeof(ViewCounters) * nj) +
              a(sizeof(float4) * nv_mv) + a(sizeof(float4) * kPlaneStride * next) +
              a(sizeof(uint32_t) * nblk) + a(sizeof(uint32_t) * next) + a(sizeof(uint4) * next) +
-             a(sizeof(uint32_t) * pix);
+             a(sizeof(RayStart) * pix);
   if (mode == VFR_MODE_REF) t += a(sizeof(int32_t) * pix);
   if (mode == VFR_MODE_COMPOSITED)
     t += 2 * a(sizeof(uint32_t) * pix) + 2 * a(sizeof(uint32_t) * (stiles + 1)) +
@@ -312,7 +312,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
   if (!rc) rc = place(blk, sizeof(uint32_t) * nblk, "block counts");
   if (!rc) rc = place(vis, sizeof(uint32_t) * next, "visible lists");
   if (!rc) rc = place(bbox, sizeof(uint4) * next, "bboxes");
-  if (!rc) rc = place(rays, sizeof(uint32_t) * pix, "ray lists");
+  if (!rc) rc = place(rays, sizeof(RayStart) * pix, "ray lists");
   if (!rc && mode == VFR_MODE_REF) rc = place(winner, sizeof(int32_t) * pix, "winner maps");
   if (!rc && mode == VFR_MODE_COMPOSITED) {
     if (ent_cap == 0) ent_cap = (C.ent_cap_hint && !arena) ? C.ent_cap_hint : pix * 4 + 1024;
@@ -360,7 +360,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     J.vis_ext = vis.as<uint32_t>(sizeof(uint32_t) * oe);
     J.bbox = bbox.as<uint4>(sizeof(uint4) * oe);
     J.winner = mode == VFR_MODE_REF ? winner.as<int32_t>(sizeof(int32_t) * op) : nullptr;
-    J.rays = rays.as<uint32_t>(sizeof(uint32_t) * op);
+    J.rays = rays.as<RayStart>(sizeof(RayStart) * op);
     J.ent_cnt = mode == VFR_MODE_COMPOSITED ? ent_cnt.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
     J.ent_off = mode == VFR_MODE_COMPOSITED ? ent_off.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
     J.ctr = d_ctr.as<ViewCounters>(sizeof(ViewCounters) * j);

@@ -136,28 +136,36 @@ __device__ __forceinline__ WalkRec ldg_walk(const WalkRec* w, uint32_t t) {
   return r;
 }
 
+// Start a segment in tet t through its face f, with entry depth zp and the
+// back colour's transfer-function entry cbi (:256-279).  False (checked build
+// only): the tet or one of its vertex ids is out of range, and nothing was
+// loaded.
+__device__ __forceinline__ bool begin_segment_at(const JobDev& J, Ray& R, uint32_t t, uint32_t f,
+                                                 float zp, uint32_t cbi) {
+  if (id_bad(t, J.nT)) return false;
+  R.t = t;
+  R.f = f;
+  const uint4 id = __ldg(J.tet + t);
+  if (id_bad(id.x, J.nV) || id_bad(id.y, J.nV) || id_bad(id.z, J.nV) || id_bad(id.w, J.nV))
+    return false;
+  R.w = ldg_walk(R.walk, t);
+  R.r0 = __ldg(R.vert + sel4(id, f));
+  R.r1 = __ldg(R.vert + sel4(id, (f + 1) & 3u));
+  R.r2 = __ldg(R.vert + sel4(id, (f + 2) & 3u));
+  R.r3 = __ldg(R.vert + sel4(id, (f + 3) & 3u));
+  R.zp = zp;
+  R.lastZ = zp;
+  R.cbi = cbi;
+  s_watch_saved[threadIdx.x] = 0xffffffffu;  // a new segment walks other states
+  return true;
+}
+
 // Start a segment at external face e (in range: the caller read its plane)
-// with entry depth zp (:256-279).  False (checked build only): the face's
-// tet or one of its vertex ids is out of range, and nothing was loaded.
+// with entry depth zp and entry scalar sp.
 __device__ __forceinline__ bool begin_segment(const JobDev& J, Ray& R, uint32_t e, float zp,
                                               float sp) {
   const uint2 tf = __ldg(J.extf + e);
-  if (id_bad(tf.x, J.nT)) return false;
-  R.t = tf.x;
-  R.f = tf.y;
-  const uint4 id = __ldg(J.tet + R.t);
-  if (id_bad(id.x, J.nV) || id_bad(id.y, J.nV) || id_bad(id.z, J.nV) || id_bad(id.w, J.nV))
-    return false;
-  R.w = ldg_walk(R.walk, R.t);
-  R.r0 = __ldg(R.vert + sel4(id, R.f));
-  R.r1 = __ldg(R.vert + sel4(id, (R.f + 1) & 3u));
-  R.r2 = __ldg(R.vert + sel4(id, (R.f + 2) & 3u));
-  R.r3 = __ldg(R.vert + sel4(id, (R.f + 3) & 3u));
-  R.zp = zp;
-  R.lastZ = zp;
-  R.cbi = (uint32_t)fmul(255.0f, sp);
-  s_watch_saved[threadIdx.x] = 0xffffffffu;  // a new segment walks other states
-  return true;
+  return begin_segment_at(J, R, tf.x, tf.y, zp, (uint32_t)fmul(255.0f, sp));
 }
 
 // Composited mode: the pixel's next entry in its list, which stage (b)
@@ -419,7 +427,9 @@ __device__ __forceinline__ uint32_t step(const TraverseParams& P, const SharedTa
 
 // Start the ray of the job's local ray index `local`: its pixel, the
 // pixel's object coordinates, and its first segment -- the winning entry
-// face (reference mode) or the first entry of the pixel's list (composited
+// face's, from the start record stage (b) wrote (reference mode: three
+// levels of dependent loads, the record, then the tet and its walk record,
+// then the vertices), or the first entry of the pixel's list (composited
 // mode; kMode 2 takes the mode from the job).  Returns whether the ray
 // walks; a composited pixel without a usable entry is finished here.
 template <int kMode>
@@ -431,7 +441,8 @@ __device__ __forceinline__ bool start_ray(const TraverseParams& P, const JobDev&
   R.nV = J.nV;
   R.watch = min(kWatchSteps, step_cap_of(P, J.nT));
   R.rmaxEdge = __drcp_rn((double)job_maxedge(J));
-  R.p = J.rays[local];
+  const RayStart rs = J.rays[local];
+  R.p = rs.p;
   if (id_bad(R.p, J.W * J.H)) {
     status |= kDevRange;
     return false;
@@ -443,16 +454,8 @@ __device__ __forceinline__ bool start_ray(const TraverseParams& P, const JobDev&
   R.tr = 1.0f;
   R.iters = 0;
   const bool ref = kMode == 0 || (kMode == 2 && J.mode == 0);
-  if (ref) {
-    const uint32_t e = (uint32_t)J.winner[R.p];
-    if (id_bad(e, J.nExt)) {
-      status |= kDevRange;
-      return false;
-    }
-    const float4 p0 = J.planes[kPlaneStride * (size_t)e];
-    const float4 p1 = J.planes[kPlaneStride * (size_t)e + 1];
-    if (!begin_segment(J, R, e, plane_eval(R.ox, R.oy, p0.x, p0.y, p0.z),
-                       plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y))) {
+  if (ref) {  // stage (b) resolved the winning face's segment start
+    if (!begin_segment_at(J, R, rs.tf >> 2, rs.tf & 3u, __uint_as_float(rs.zp), rs.cbi)) {
       status |= kDevRange;
       return false;
     }

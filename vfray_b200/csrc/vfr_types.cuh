@@ -19,6 +19,15 @@ struct __align__(16) ViewCounters {
 };
 
 // One job as the kernels see it (device memory, uploaded with the batch).
+// A ray's start, written by stage (b) when it lists the rays: the pixel and,
+// in reference mode, the winning face's tet and entry face (tet << 2 |
+// face), the entry depth (float bits) and the back colour's
+// transfer-function entry.  The traversal starts a ray from it without going
+// back through the winner map, the face's plane and the external-face list.
+struct __align__(16) RayStart {
+  uint32_t p, tf, zp, cbi;
+};
+
 struct __align__(16) JobDev {
   float4 m0, m1, m2;         // rows of the model-view (use_mv)
   const uint4* tet;          // mesh
@@ -34,7 +43,7 @@ struct __align__(16) JobDev {
   uint32_t* vis_ext;         // visible external faces, in order
   uint4* bbox;               // per visible face
   int32_t* winner;           // W*H, reference mode
-  uint32_t* rays;            // W*H capacity
+  RayStart* rays;            // W*H capacity
   uint32_t* ent_cnt;         // composited: W*H entry counts
   uint32_t* ent_off;         // composited: W*H offsets of the pixels' lists in ent
   const uint2* ent;          // composited: the batch's entry arena (z bits, ext face),
