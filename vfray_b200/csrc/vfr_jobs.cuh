@@ -520,12 +520,13 @@ __global__ void __launch_bounds__(256) bin_kernel(const JobDev* __restrict__ job
 }
 
 // A face as the tile kernel tests it: its box, entry edges, depth and
-// scalar planes, ext-face index.
+// scalar planes, ext-face index, and the tet and entry face a segment
+// starting at it enters (tet << 2 | face).
 struct TileFace {
   uint4 box;
   EntryEdges E;
   float zx, zy, zz, sx, sy, sz;
-  uint32_t e;
+  uint32_t e, tf;
 };
 
 // One CTA per screen tile (a block-stride loop over the tiles of all jobs),
@@ -541,7 +542,7 @@ __global__ void __launch_bounds__(256) tile_kernel(const JobDev* __restrict__ jo
                                                    const uint32_t* __restrict__ tpref,
                                                    const uint32_t* __restrict__ tile_off,
                                                    const uint32_t* __restrict__ bins,
-                                                   uint32_t bin_cap, uint2* __restrict__ ent,
+                                                   uint32_t bin_cap, uint4* __restrict__ ent,
                                                    uint32_t ent_cap, uint32_t* __restrict__ cursor) {
   __shared__ TileFace F[256];
   __shared__ uint32_t s_warp[8];
@@ -589,6 +590,8 @@ __global__ void __launch_bounds__(256) tile_kernel(const JobDev* __restrict__ jo
         f.sy = p1.x;
         f.sz = p1.y;
         f.e = e;
+        const uint2 tf = J.extf[e];
+        f.tf = (tf.x << 2) | (tf.y & 3u);
         F[tid] = f;
       }
       __syncthreads();
@@ -652,17 +655,21 @@ __global__ void __launch_bounds__(256) tile_kernel(const JobDev* __restrict__ jo
     }
     // pass 2: each pixel's entries, inserted in descending (depth, face) order
     uint32_t n = 0;
+    // each entry also carries what its segment starts from (the face's tet
+    // and entry face, the back colour's TF entry), so the traversal starts a
+    // segment without going back through the plane and the external face
     auto insert = [&](const TileFace& f) {
       const float z = plane_eval(ox, oy, f.zx, f.zy, f.zz);
+      const uint32_t cbi = (uint32_t)fmul(255.0f, plane_eval(ox, oy, f.sx, f.sy, f.sz));
       uint32_t q = n++;
       while (q > 0) {
-        const uint2 a = ent[off + q - 1];
+        const uint4 a = ent[off + q - 1];
         const float za = __uint_as_float(a.x);
         if (za > z || (za == z && a.y > f.e)) break;
         ent[off + q] = a;
         --q;
       }
-      ent[off + q] = make_uint2(__float_as_uint(z), f.e);
+      ent[off + q] = make_uint4(__float_as_uint(z), f.e, f.tf, cbi);
     };
     if (one_chunk) {  // F still holds the chunk pass 1 staged
       if (live && fits && count) {

@@ -243,7 +243,7 @@ size_t Batch::arena_bytes(Ctx& C, const std::vector<JobSpec>& s, int mode, uint3
   if (mode == VFR_MODE_COMPOSITED)
     t += 2 * a(sizeof(uint32_t) * pix) + 2 * a(sizeof(uint32_t) * (stiles + 1)) +
          a(sizeof(uint32_t) * stiles) + a(sizeof(uint32_t) * (cdiv(stiles + 1, fb) + 1)) +
-         a(sizeof(uint32_t) * (32 * stiles + 4 * next)) + a(sizeof(uint2) * (pix * 4 + 1024));
+         a(sizeof(uint32_t) * (32 * stiles + 4 * next)) + a(sizeof(uint4) * (pix * 4 + 1024));
   t += a(3 * pix);
   if (!rgb8_only) t += a(sizeof(float4) * pix) + a(sizeof(uint32_t) * pix);
   return t;
@@ -325,7 +325,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     if (!rc) rc = place(tile_cur, sizeof(uint32_t) * stiles, "tile cursors");
     if (!rc) rc = place(scan, sizeof(uint32_t) * (cdiv(stiles + 1, fb) + 1), "scan sums");
     if (!rc) rc = place(bins, sizeof(uint32_t) * bin_cap, "tile bins");
-    if (!rc) rc = place(ent, sizeof(uint2) * ent_cap, "entries");
+    if (!rc) rc = place(ent, sizeof(uint4) * ent_cap, "entries");
   }
   if (!rc && own_outputs) {
     rc = place(out_rgb8, 3 * pix, "rgb8 outputs");
@@ -364,7 +364,7 @@ int Batch::layout(const std::vector<JobSpec>& s, int m, bool own_outputs) {
     J.ent_cnt = mode == VFR_MODE_COMPOSITED ? ent_cnt.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
     J.ent_off = mode == VFR_MODE_COMPOSITED ? ent_off.as<uint32_t>(sizeof(uint32_t) * op) : nullptr;
     J.ctr = d_ctr.as<ViewCounters>(sizeof(ViewCounters) * j);
-    J.ent = mode == VFR_MODE_COMPOSITED ? ent.as<uint2>() : nullptr;
+    J.ent = mode == VFR_MODE_COMPOSITED ? ent.as<uint4>() : nullptr;
     J.ent_cap = (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu);
     J.mode = (uint32_t)mode;
     if (own_outputs) {
@@ -484,7 +484,7 @@ int Batch::enqueue_b() {
                                          tile_cur.as<uint32_t>(), bins.as<uint32_t>(), bcap);
     if (stiles)
       tile_kernel<<<std::min<uint32_t>(stiles, (uint32_t)C.num_sms * 8), 256, 0, st>>>(
-          J, njobs, ps, tile_off.as<uint32_t>(), bins.as<uint32_t>(), bcap, ent.as<uint2>(),
+          J, njobs, ps, tile_off.as<uint32_t>(), bins.as<uint32_t>(), bcap, ent.as<uint4>(),
           (uint32_t)std::min<size_t>(ent_cap, 0xffffffffu), queue() + 1);
   }
   if (tiles) raylist_kernel<<<cdiv(tiles, 8), 256, 0, st>>>(J, njobs, P + 3 * n1, mode, tile_w);

@@ -160,13 +160,6 @@ __device__ __forceinline__ bool begin_segment_at(const JobDev& J, Ray& R, uint32
   return true;
 }
 
-// Start a segment at external face e (in range: the caller read its plane)
-// with entry depth zp and entry scalar sp.
-__device__ __forceinline__ bool begin_segment(const JobDev& J, Ray& R, uint32_t e, float zp,
-                                              float sp) {
-  const uint2 tf = __ldg(J.extf + e);
-  return begin_segment_at(J, R, tf.x, tf.y, zp, (uint32_t)fmul(255.0f, sp));
-}
 
 // Composited mode: the pixel's next entry in its list, which stage (b)
 // wrote in descending (depth, face) order, skipping entries above the depth
@@ -180,16 +173,13 @@ __device__ __forceinline__ bool next_entry(const TraverseParams& P, const JobDev
       bad = true;
       break;
     }
-    const uint2 q = J.ent[R.ea + R.de];
+    const uint4 q = J.ent[R.ea + R.de];
     ++R.de;
     const float z = __uint_as_float(q.x);
     if (z > R.exitZ) continue;  // behind the ray already
-    if (id_bad(q.y, J.nExt)) {
-      bad = true;
-      break;
-    }
-    const float4 p0 = J.planes[kPlaneStride * (size_t)q.y], p1 = J.planes[kPlaneStride * (size_t)q.y + 1];
-    if (begin_segment(J, R, q.y, z, plane_eval(R.ox, R.oy, p0.w, p1.x, p1.y))) return true;
+    // stage (b) resolved the segment's start: tet << 2 | entry face, and the
+    // back colour's transfer-function entry
+    if (begin_segment_at(J, R, q.z >> 2, q.z & 3u, z, q.w)) return true;
     bad = true;
     break;
   }

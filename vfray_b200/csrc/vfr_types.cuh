@@ -46,8 +46,9 @@ struct __align__(16) JobDev {
   RayStart* rays;            // W*H capacity
   uint32_t* ent_cnt;         // composited: W*H entry counts
   uint32_t* ent_off;         // composited: W*H offsets of the pixels' lists in ent
-  const uint2* ent;          // composited: the batch's entry arena (z bits, ext face),
-                             // each pixel's list in descending (depth, face) order
+  const uint4* ent;          // composited: the batch's entry arena (z bits, ext face,
+                             // tet << 2 | entry face, back-colour TF entry), each
+                             // pixel's list in descending (depth, face) order
   uint32_t ent_cap;          // its capacity in entries
   ViewCounters* ctr;
   uint8_t* rgb8;             // outputs (any may be null)
